@@ -1,0 +1,161 @@
+// gd_device.cuh -- device building blocks of the REMC docking kernels:
+// counter-based RNG, the bit-reproducible decision exp, and the mbarrier /
+// bulk-copy (TMA engine, non-tensor) primitives for sm_100a.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gd {
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).  Stream layout:
+//   key  = { seed_lo, seed_hi ^ stream_id }
+//   move of replica r at MC step s:      ctr {r, s, 0, 0} -> perturbations 0..3
+//                                        ctr {r, s, 1, 0} -> perturbations 4..5,
+//                                                            word 2: accept u
+//   exchange round k, group g, pair j:   ctr {g, k, 2, j} -> word 0
+// ---------------------------------------------------------------------------
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const uint32_t hi0 = mulhi32(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+__host__ __device__ __forceinline__ void rng_key(uint64_t seed, uint32_t stream, uint32_t &k0,
+                                                 uint32_t &k1) {
+  k0 = (uint32_t)seed;
+  k1 = (uint32_t)(seed >> 32) ^ stream;
+}
+
+// 24-bit uniform in [0, 1); exact in single precision.
+__device__ __forceinline__ float u01(uint32_t x) {
+  return __fmul_rn(__uint2float_rn(x >> 8), 0x1p-24f);
+}
+
+// ---------------------------------------------------------------------------
+// Decision exp: Cody-Waite reduction with ln 2 split in a 16-bit head and a
+// tail, degree-7 Taylor polynomial of e^r on |r| <= ln2/2 (Horner, fused),
+// scaling by 2^k in two exact multiplies.  Each step is one correctly
+// rounded IEEE operation, so the host oracle's copy returns the same bits.
+// Used only where a decision is taken (Metropolis, exchange); the energy uses
+// the hardware exp2.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float decision_expf(float x) {
+  if (x != x) return x;
+  if (x > 88.72f) return __int_as_float(0x7f800000);
+  if (x < -87.33f) return 0.0f;
+  const float kf = rintf(__fmul_rn(x, 0x1.715476p+0f));
+  float r = __fmaf_rn(-kf, 0x1.62e400p-1f, x);
+  r = __fmaf_rn(-kf, 0x1.7f7d1cp-20f, r);
+  float p = 0x1.a01a02p-13f;
+  p = __fmaf_rn(p, r, 0x1.6c16c2p-10f);
+  p = __fmaf_rn(p, r, 0x1.111112p-7f);
+  p = __fmaf_rn(p, r, 0x1.555556p-5f);
+  p = __fmaf_rn(p, r, 0x1.555556p-3f);
+  p = __fmaf_rn(p, r, 0x1.0p-1f);
+  p = __fmaf_rn(p, r, 1.0f);
+  p = __fmaf_rn(p, r, 1.0f);
+  const int k = (int)kf;
+  const int k1 = k / 2, k2 = k - k1;
+  const float s1 = __int_as_float((k1 + 127) << 23);
+  const float s2 = __int_as_float((k2 + 127) << 23);
+  return __fmul_rn(__fmul_rn(p, s1), s2);
+}
+
+// Metropolis rule (accept_d.cu:19-23) on given totals.
+__device__ __forceinline__ int metropolis(float e_new, float e_old, float minus_beta, float u) {
+  const float de = __fsub_rn(e_new, e_old);
+  return u < decision_expf(__fmul_rn(de, minus_beta)) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory mbarrier and bulk async copy (cp.async.bulk, TMA engine,
+// plain 1-D form: no tensor map, no multicast).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls (each try_wait itself blocks for
+// a hardware-defined slice), records `code` in *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          uint32_t limit = (1u << 22)) {
+  for (uint32_t i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicExch(err, code);
+  return false;
+}
+
+// Global -> shared bulk copy completing on an mbarrier (bytes % 16 == 0,
+// both addresses 16-byte aligned).
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Barrier over the compute warps only (the producer warp never joins).
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+}  // namespace gd

@@ -1,0 +1,263 @@
+"""ctypes binding of libgpudock.so (the C-ABI of include/gpudock.h).
+
+The library is built in-tree by :mod:`gpudock_b200.build`; loading it never
+falls back to anything else: a missing or unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libgpudock.so")
+
+_lib = None
+
+
+class GdError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        self.status = status
+        super().__init__(f"{where}: {abi.STATUS.get(status, status)}: {msg}")
+
+
+def _declare(lib):
+    P = C.c_void_p
+    i32, u32, u64 = C.c_int, C.c_uint32, C.c_uint64
+    sigs = {
+        "gd_last_error": ([], C.c_char_p),
+        "gd_version": ([], C.c_char_p),
+        "gd_enepara_optimize": ([C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara)], i32),
+        "gd_set_temperature": ([i32, C.c_float, C.c_float, abi.f32p, abi.f32p], i32),
+        "gd_complex_validate": ([C.POINTER(abi.GdComplex)], i32),
+        "gd_ctx_create": ([i32, P, C.POINTER(P)], i32),
+        "gd_ctx_destroy": ([P], i32),
+        "gd_ctx_sync": ([P], i32),
+        "gd_ctx_launch_count": ([P], u64),
+        "gd_complex_upload": ([P, C.POINTER(abi.GdComplex), C.POINTER(P)], i32),
+        "gd_complex_free": ([P], i32),
+        "gd_complex_device_bytes": ([P], C.c_size_t),
+        "gd_energy_poses_dev": ([P, P, i32, i32, i32, P, P, P], i32),
+        "gd_energy_poses": ([P, P, i32, i32, i32, abi.f32p, abi.f32p, abi.f64p], i32),
+        "gd_remc_create": ([P, P, C.POINTER(abi.GdMcParams), C.POINTER(P)], i32),
+        "gd_remc_init": ([P], i32),
+        "gd_remc_run": ([P, i32], i32),
+        "gd_remc_read": ([P, C.POINTER(abi.GdMcLog)], i32),
+        "gd_remc_destroy": ([P], i32),
+        "gd_remc_n_rep": ([P], i32),
+        "gd_remc_set_profiling": ([P, i32], i32),
+        "gd_remc_kernel_times": ([P, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_int)], i32),
+        "gd_run": ([C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams), C.POINTER(abi.GdMcLog)], i32),
+        "gd_metropolis_dev": ([P, i32, P, P, P, P, P, u64, u32, P], i32),
+        "gd_philox_dev": ([P, i32, P, P, P], i32),
+        "gd_expf_dev": ([P, i32, P, P], i32),
+        "gd_fma_peak": ([P, i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_double)], i32),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.argtypes = args
+        fn.restype = res
+
+
+def load(path: str = LIB_PATH):
+    """Loads libgpudock.so (building it first when the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path) or os.environ.get("GD_REBUILD"):
+        from . import build
+        build.build()
+    lib = C.CDLL(path)
+    _declare(lib)
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().gd_last_error().decode(errors="replace")
+
+
+def check(status: int, where: str):
+    if status != abi.GD_OK:
+        raise GdError(status, where, last_error())
+
+
+# ---------------------------------------------------------------------------
+# Host-side helpers (no GPU needed)
+# ---------------------------------------------------------------------------
+def enepara_optimize(raw: abi.GdEneparaRaw) -> abi.GdEnepara:
+    out = abi.GdEnepara()
+    check(load().gd_enepara_optimize(C.byref(raw), C.byref(out)), "gd_enepara_optimize")
+    return out
+
+
+def set_temperature(n: int, floor_t: float, ceil_t: float):
+    t = np.zeros(n, np.float32)
+    mb = np.zeros(n, np.float32)
+    check(load().gd_set_temperature(n, floor_t, ceil_t, abi._ptr(t, C.c_float),
+                                    abi._ptr(mb, C.c_float)), "gd_set_temperature")
+    return t, mb
+
+
+def validate(cx: abi.Complex) -> int:
+    return load().gd_complex_validate(C.byref(cx.struct()))
+
+
+# ---------------------------------------------------------------------------
+# Device objects
+# ---------------------------------------------------------------------------
+class Context:
+    """A CUDA device + stream bound to the library (gd_ctx)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.gd_ctx_create(device, C.c_void_p(stream) if stream else None,
+                                      C.byref(h)), "gd_ctx_create")
+        self.h = h
+
+    def sync(self):
+        check(self._lib.gd_ctx_sync(self.h), "gd_ctx_sync")
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.gd_ctx_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            self._lib.gd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class DeviceComplex:
+    """A complex uploaded to the device in the kernel layout (gd_dcomplex)."""
+
+    def __init__(self, ctx: Context, cx: abi.Complex):
+        self.ctx = ctx
+        self.cx = cx
+        h = C.c_void_p()
+        check(ctx._lib.gd_complex_upload(ctx.h, C.byref(cx.struct()), C.byref(h)),
+              "gd_complex_upload")
+        self.h = h
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.ctx._lib.gd_complex_device_bytes(self.h))
+
+    def energy_poses(self, poses: np.ndarray, prt_conf: int = 0, lig_conf: int = 0,
+                     raw: bool = True):
+        """Host-buffer call: terms [n, 10] float32 and raw [n, 9] float64."""
+        poses = np.ascontiguousarray(poses, np.float32).reshape(-1, 6)
+        n = poses.shape[0]
+        terms = np.zeros((n, abi.NTERM), np.float32)
+        rw = np.zeros((n, abi.NRAW), np.float64) if raw else None
+        check(self.ctx._lib.gd_energy_poses(
+            self.ctx.h, self.h, prt_conf, lig_conf, n, abi._ptr(poses, C.c_float),
+            abi._ptr(terms, C.c_float), abi._ptr(rw, C.c_double)), "gd_energy_poses")
+        return terms, rw
+
+    def energy_poses_dev(self, n: int, poses_ptr: int, terms_ptr: int, raw_ptr: int = 0,
+                         prt_conf: int = 0, lig_conf: int = 0):
+        """Device-pointer call (asynchronous on the context stream)."""
+        check(self.ctx._lib.gd_energy_poses_dev(
+            self.ctx.h, self.h, prt_conf, lig_conf, n, C.c_void_p(poses_ptr),
+            C.c_void_p(terms_ptr), C.c_void_p(raw_ptr) if raw_ptr else None),
+            "gd_energy_poses_dev")
+
+    def close(self):
+        if self.h:
+            self.ctx._lib.gd_complex_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Remc:
+    """Replica-exchange Monte Carlo of one uploaded complex (gd_remc)."""
+
+    def __init__(self, dcx: DeviceComplex, steps_total: int, steps_per_exchange: int,
+                 minus_beta, move_scale=(0.02, 0.02, 0.02, 0.08, 0.08, 0.08), seed: int = 1,
+                 stream_id: int = 0, flags: int = abi.MC_EXCHANGE, steps_per_dump: int = 1000):
+        self.dcx = dcx
+        self.params, self._mb = abi.mc_params(steps_total, steps_per_exchange, minus_beta,
+                                              move_scale, seed, stream_id, flags, steps_per_dump)
+        h = C.c_void_p()
+        lib = dcx.ctx._lib
+        check(lib.gd_remc_create(dcx.ctx.h, dcx.h, C.byref(self.params), C.byref(h)),
+              "gd_remc_create")
+        self.h = h
+        self.n_rep = int(lib.gd_remc_n_rep(h))
+        self.n_tmp = int(self.params.n_tmp)
+        self.steps_total = int(steps_total)
+        self.record = bool(flags & abi.MC_RECORD)
+
+    def init(self):
+        check(self.dcx.ctx._lib.gd_remc_init(self.h), "gd_remc_init")
+
+    def run(self, n_steps: int):
+        check(self.dcx.ctx._lib.gd_remc_run(self.h, int(n_steps)), "gd_remc_run")
+
+    def set_profiling(self, on: bool = True):
+        check(self.dcx.ctx._lib.gd_remc_set_profiling(self.h, int(on)), "gd_remc_set_profiling")
+
+    def kernel_times(self):
+        """(MC-interval ms, launches, exchange ms, launches) since the last call."""
+        a, b = C.c_double(), C.c_double()
+        na, nb = C.c_int(), C.c_int()
+        check(self.dcx.ctx._lib.gd_remc_kernel_times(self.h, C.byref(a), C.byref(na), C.byref(b),
+                                                     C.byref(nb)), "gd_remc_kernel_times")
+        return a.value, na.value, b.value, nb.value
+
+    def read(self) -> abi.McLogBuffers:
+        buf = abi.McLogBuffers(self.n_rep, self.n_tmp, self.steps_total, self.record)
+        check(self.dcx.ctx._lib.gd_remc_read(self.h, C.byref(buf.log)), "gd_remc_read")
+        return buf
+
+    def close(self):
+        if self.h:
+            self.dcx.ctx._lib.gd_remc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run(cx: abi.Complex, steps_total: int, steps_per_exchange: int, minus_beta, **kw):
+    """gd_run: the one-call counterpart of the reference's Run()."""
+    params, mb = abi.mc_params(steps_total, steps_per_exchange, minus_beta, **kw)
+    n_rep = cx.n_prt * cx.n_lig * len(mb)
+    buf = abi.McLogBuffers(n_rep, len(mb), steps_total, bool(params.flags & abi.MC_RECORD))
+    check(load().gd_run(C.byref(cx.struct()), C.byref(params), C.byref(buf.log)), "gd_run")
+    return buf
+
+
+def fma_peak(ctx: Context, n_blocks: int = 148 * 16, iters: int = 4096):
+    ms = C.c_float()
+    fl = C.c_double()
+    check(ctx._lib.gd_fma_peak(ctx.h, n_blocks, iters, C.byref(ms), C.byref(fl)), "gd_fma_peak")
+    return fl.value / (ms.value * 1e-3)

@@ -1,0 +1,335 @@
+/*
+ * gpudock.h -- C-ABI of the B200 replica-exchange Monte Carlo (REMC)
+ * docking path of GeauxDock / gpudocksm.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or
+ * torch types.  Host buffers are owned by the caller; device memory is owned
+ * by the opaque handles (gd_ctx, gd_dcomplex, gd_remc, gd_batch, gd_server).
+ * Every call returns gd_status; nothing calls exit().
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   Run()            gpudocksm-rem-1.2/src/run.h:6-17, run.cu:41-353
+ *   MonteCarlo_d     gpudocksm-rem-1.2/src/montecarlo_d.cu:59-104
+ *   CalcEnergy_d     gpudocksm-rem-1.2/src/calcenergy_d.cu:22-374
+ *   ExchangeReplicas gpudocksm-rem-1.2/src/exchangereplicas_d.cu:7-139
+ *   OptimizeEnepara  gpudocksm-rem-1.2/src/util.C:405-458
+ *   SetTemperature   gpudocksm-rem-1.2/src/util.C:491-532
+ *   SetReplica       gpudocksm-rem-1.2/src/util.C:538-558
+ */
+#ifndef GPUDOCK_H
+#define GPUDOCK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                             */
+/* ------------------------------------------------------------------------ */
+typedef enum gd_status {
+  GD_OK = 0,
+  GD_EINVAL = 1,      /* malformed input: sizes, types, indices, NULLs     */
+  GD_ENOMEM = 2,      /* host or device allocation failed                   */
+  GD_EBUDGET = 3,     /* request larger than the server's HBM budget        */
+  GD_ECUDA = 4,       /* a CUDA runtime call failed (see gd_last_error)     */
+  GD_ETIMEDOUT = 5,   /* a bounded wait ran out                             */
+  GD_ECANCELLED = 6,  /* request cancelled before it finished               */
+  GD_ENOTFOUND = 7,   /* unknown request id                                 */
+  GD_EAGAIN = 8,      /* not finished yet (poll again)                      */
+  GD_ENODEV = 9       /* no CUDA device / kernel image not loadable         */
+} gd_status;
+
+/* Thread-local text of the last error raised on this thread. */
+const char *gd_last_error(void);
+/* Library version string. */
+const char *gd_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Force-field type space: the reference's size.h constants MAXTP1..MAXTP4, */
+/* MAXWEI (gpudocksm-rem-1.2/src/size.h:53-75).  These size the parameter   */
+/* tables, not the problem, so they stay fixed.                             */
+/* ------------------------------------------------------------------------ */
+#define GD_NPT 30    /* protein effective-point types (MAXTP1)  */
+#define GD_NLT 24    /* ligand atom types (MAXTP2)              */
+#define GD_NELE 50   /* electrostatic classes (MAXTP3)          */
+#define GD_NRES 20   /* residue types (MAXTP4)                  */
+#define GD_NTERM 10  /* energy terms incl. total (MAXWEI)       */
+#define GD_NRAW 9    /* un-normalised terms returned in FP64    */
+
+/* MCS coordinate that marks an absent atom (size.h:97). */
+#define GD_MCS_INVALID_COORD 728492.0f
+
+/* Energy term order inside a 10-float energy record: the rem order of
+ * calcenergy_d.cu:301-309 and dock.h:98-116. */
+enum {
+  GD_E_VDW = 0, GD_E_ELE = 1, GD_E_PMF = 2, GD_E_PSP = 3, GD_E_HDB = 4,
+  GD_E_HPC = 5, GD_E_KDE = 6, GD_E_LHM = 7, GD_E_DST = 8, GD_E_TOTAL = 9
+};
+
+/* Raw force field as loaded from the .ff parameter file
+ * (EnePara0, gpudocksm-rem-1.2/src/dock.h:363-379). */
+typedef struct gd_enepara_raw {
+  float vdw[GD_NPT][GD_NLT][2];
+  float ele[GD_NELE];
+  float pmf[GD_NPT][GD_NLT][2];
+  float hpp[GD_NRES];
+  float hpl[GD_NLT][2];
+  float hdb[GD_NPT][GD_NLT][2];
+  float lj[3];
+  float el[2];
+  float kde;
+  float w[GD_NTERM];
+  float a_para[GD_NTERM];
+  float b_para[GD_NTERM];
+} gd_enepara_raw;
+
+/* Kernel-ready force field (EnePara, dock.h:386-421), same field order.
+ * Build it with gd_enepara_optimize(). */
+typedef struct gd_enepara {
+  float p1a[GD_NLT][GD_NPT];
+  float p2a[GD_NLT][GD_NPT];
+  float lj0, lj1;
+  float el0;
+  float el1;
+  float ele[GD_NELE];
+  float a1;
+  float b1;
+  float pmf0[GD_NLT][GD_NPT];
+  float pmf1[GD_NLT][GD_NPT];
+  float hdb0[GD_NLT][GD_NPT];
+  float hdb1[GD_NLT][GD_NPT];
+  float hdb2[GD_NLT][GD_NPT];
+  float hpp[GD_NRES];
+  float hpl0[GD_NLT];
+  float hpl1[GD_NLT];
+  float hpl2[GD_NLT];
+  float kde2;
+  float kde3;
+  float w[GD_NTERM];
+  float a_para[GD_NTERM];
+  float b_para[GD_NTERM];
+} gd_enepara;
+
+/* Derives the kernel tables: p1a = 2 eps (s r)^9, p2a = 3 eps (s r)^6,
+ * hdb1 = 1/sigma, hpl2 = log(1/(sigma sqrt(2 pi))), kde2 = -1/(2h^2),
+ * kde3 = (h sqrt(2 pi))^3.  Replaces OptimizeEnepara (util.C:405-458). */
+gd_status gd_enepara_optimize(const gd_enepara_raw *raw, gd_enepara *out);
+
+/* Geometric temperature ladder T_i = T_floor * r^i and minus_beta = -1/T_i
+ * (k_B = 1).  n == 1 uses the floor temperature.  Replaces SetTemperature
+ * (util.C:491-532).  temps may be NULL. */
+gd_status gd_set_temperature(int n_tmp, float floor_temp, float ceiling_temp,
+                             float *temps, float *minus_beta);
+
+/* ------------------------------------------------------------------------ */
+/* Inputs (host, caller-owned).  Structure-of-arrays, no capacity caps.      */
+/* ------------------------------------------------------------------------ */
+
+/* Protein: pnp effective points, n_conf conformations.  Point properties are
+ * shared by all conformations; coordinates are per conformation.  The fields
+ * are those of Protein (dock.h:254-274) after CopyProteinResidue
+ * (util.C:253-275). */
+typedef struct gd_protein {
+  int pnp;
+  int n_conf;
+  const float *x, *y, *z;      /* [n_conf * pnp]                           */
+  const int *t;                /* [pnp] point type, 0..GD_NPT-1            */
+  const int *c;                /* [pnp] point class, 0..3                  */
+  const float *ele;            /* [pnp] ele[t == 0 ? d + 30 : t]           */
+  const int *seq3r;            /* [pnp] residue serial, index into psp row */
+  const int *c0_and_d12_or_c2; /* [pnp] (c == 0 && d == 12) || c == 2      */
+  const float *hpp;            /* [pnp] hpp[d]                             */
+  float pocket_center[3];
+} gd_protein;
+
+/* Ligand: lna atoms, n_conf conformations with coordinates relative to the
+ * ligand centre (coord_orig of Ligand, dock.h:191-216, after OptimizeLigand
+ * util.C:200-226 which sets center := pocket centre). */
+typedef struct gd_ligand {
+  int lna;
+  int n_conf;
+  const float *x, *y, *z;      /* [n_conf * lna]                           */
+  const int *t;                /* [lna] atom type, 0..GD_NLT-1             */
+  const float *c;              /* [lna] partial charge                     */
+  const int *n;                /* [lna] atom number; MCS field = n + 1     */
+  float center[3];             /* coord_orig.center                        */
+} gd_ligand;
+
+/* Pocket-specific potential psp[lig type][seq3r] (Psp, dock.h:289-295). */
+typedef struct gd_psp {
+  int n_col;                   /* row length; every seq3r must be < n_col  */
+  const float *psp;            /* [GD_NLT * n_col]                         */
+} gd_psp;
+
+/* KDE points (Kde, dock.h:317-325). */
+typedef struct gd_kde {
+  int pnk;
+  const float *x, *y, *z;      /* [pnk]                                    */
+  const int *t;                /* [pnk] ligand atom type                   */
+} gd_kde;
+
+/* LHM position restraints (Mcs, dock.h:347-354): pos MCS records of n_field
+ * coordinates each; absent atoms hold GD_MCS_INVALID_COORD. */
+typedef struct gd_mcs {
+  int pos;
+  int n_field;                 /* > max(ligand n) + 1; reference MAXMCS=256 */
+  const float *x, *y, *z;      /* [pos * n_field]                          */
+  const float *tcc;            /* [pos]                                    */
+} gd_mcs;
+
+/* One docking complex: a ligand ensemble against a protein ensemble with its
+ * pocket template and force field.  The replica grid is protein conformation
+ * x temperature x ligand conformation, flat index
+ * r = n_tmp * n_lig * p + n_lig * t + l  (SetReplica, util.C:538-558). */
+typedef struct gd_complex {
+  gd_ligand lig;
+  gd_protein prt;
+  gd_psp psp;
+  gd_kde kde;
+  gd_mcs mcs;
+  const gd_enepara *ff;
+} gd_complex;
+
+/* Checks every size, type code and index of a complex. */
+gd_status gd_complex_validate(const gd_complex *cx);
+
+/* ------------------------------------------------------------------------ */
+/* Device context and device-resident complexes                             */
+/* ------------------------------------------------------------------------ */
+typedef struct gd_ctx gd_ctx;
+typedef struct gd_dcomplex gd_dcomplex;
+
+/* Binds a CUDA device and a stream (NULL = a stream owned by the context;
+ * otherwise a cudaStream_t created by the caller on that device). */
+gd_status gd_ctx_create(int device, void *stream, gd_ctx **out);
+gd_status gd_ctx_destroy(gd_ctx *ctx);
+gd_status gd_ctx_sync(gd_ctx *ctx);
+/* Number of this library's kernels launched through ctx so far. */
+uint64_t gd_ctx_launch_count(const gd_ctx *ctx);
+
+/* Copies a complex to the device in the kernel layout (points packed into
+ * 16 B + 8 B records, type-pair table, KDE bucketed by type, MCS gathered per
+ * ligand atom).  Replaces the table staging of run.cu:114-256. */
+gd_status gd_complex_upload(gd_ctx *ctx, const gd_complex *cx,
+                            gd_dcomplex **out);
+gd_status gd_complex_free(gd_dcomplex *dcx);
+/* Device bytes held by an uploaded complex. */
+size_t gd_complex_device_bytes(const gd_dcomplex *dcx);
+
+/* ------------------------------------------------------------------------ */
+/* Pose energies (CalcEnergy_d after Move_d on a given move vector)         */
+/* ------------------------------------------------------------------------ */
+/* A pose is a 6-float move vector (tx, ty, tz, rx, ry, rz), the reference's
+ * movematrix: x = R_zyx(rx, ry, rz) * x_orig + t + centre (move_d.cu:86-127).
+ * terms: [n_pose][GD_NTERM] normalised terms + weighted total (FP32).
+ * raw:   [n_pose][GD_NRAW] un-normalised terms in FP64 (may be NULL).
+ * The _dev form takes device pointers and runs on the context stream without
+ * synchronising; the host form copies poses in and results out. */
+gd_status gd_energy_poses_dev(gd_ctx *ctx, const gd_dcomplex *dcx,
+                              int prt_conf, int lig_conf, int n_pose,
+                              const float *poses_dev, float *terms_dev,
+                              double *raw_dev);
+gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *dcx, int prt_conf,
+                          int lig_conf, int n_pose, const float *poses,
+                          float *terms, double *raw);
+
+/* ------------------------------------------------------------------------ */
+/* Replica-exchange Monte Carlo                                             */
+/* ------------------------------------------------------------------------ */
+#define GD_MC_EXCHANGE   0x1u  /* temperature exchange (IS_EXCHANGE)        */
+#define GD_MC_MOVE_AWAY  0x2u  /* initial MoveAway_d + forced accept        */
+#define GD_MC_RECORD     0x4u  /* per-step trajectory record (IS_OUTPUT)    */
+
+typedef struct gd_mc_params {
+  int steps_total;           /* MC steps per replica                        */
+  int steps_per_exchange;    /* MC steps between exchanges                  */
+  int steps_per_dump;        /* the exchange parity restarts every dump     */
+                             /* (gpusingle.cu:14-18); <= 0 means never      */
+  int n_tmp;                 /* temperatures per (prt, lig) group           */
+  float move_scale[6];       /* translation x y z, rotation x y z           */
+  const float *minus_beta;   /* [n_tmp] -1/T per temperature index          */
+  uint64_t seed;             /* Philox4x32-10 key                           */
+  uint32_t stream_id;        /* second key word (request id when serving)   */
+  uint32_t flags;            /* GD_MC_*                                     */
+} gd_mc_params;
+
+/* Per-step trajectory record: the fields of LigRecordSingleStep
+ * (dock.h:487-493), i.e. the accepted state at the start of each step, plus
+ * the proposed total energy of that step and the Metropolis decision, so a
+ * run can be replayed decision by decision. */
+typedef struct gd_record {
+  int idx_rep, idx_prt, idx_tmp, idx_lig;
+  float e[GD_NTERM];
+  float cmcc;
+  float movematrix[6];
+  int step;
+  float e_prop_total;
+  int accepted;
+} gd_record;
+
+/* Results, the fields of McLog (dock.h:472-482) plus the final state.  Every
+ * pointer may be NULL; sizes are those of the run. */
+typedef struct gd_mc_log {
+  double t_compute;          /* seconds of device time in MC + exchange     */
+  double t_wall;             /* seconds including copies                    */
+  int64_t ac_mc;             /* accepted MC moves, all replicas             */
+  int64_t ac_temp_exchg;     /* accepted exchanges (2 per swap)             */
+  int *acs_mc;               /* [n_rep]                                     */
+  int *acs_temp_exchg;       /* [n_tmp] counted by slot t as                */
+                             /* exchangereplicas_d.cu:63-64 does            */
+  float *energy;             /* [n_rep][GD_NTERM] accepted energy           */
+  float *movematrix;         /* [n_rep][6] accepted move vector             */
+  int *idx_tmp;              /* [n_rep] temperature index of each replica   */
+  gd_record *record;         /* [n_rep][steps_total] with GD_MC_RECORD      */
+} gd_mc_log;
+
+typedef struct gd_remc gd_remc;
+
+gd_status gd_remc_create(gd_ctx *ctx, const gd_dcomplex *dcx,
+                         const gd_mc_params *mc, gd_remc **out);
+/* MonteCarlo_Init_d (montecarlo_d.cu:12-55): optional move-away with forced
+ * accept, initial energies, counters zeroed, step counter reset. */
+gd_status gd_remc_init(gd_remc *remc);
+/* Runs n_steps MC steps of every replica with an exchange after every
+ * steps_per_exchange steps (n_steps must be a multiple of it). Asynchronous. */
+gd_status gd_remc_run(gd_remc *remc, int n_steps);
+gd_status gd_remc_read(gd_remc *remc, gd_mc_log *log);
+gd_status gd_remc_destroy(gd_remc *remc);
+int gd_remc_n_rep(const gd_remc *remc);
+/* Per-launch CUDA-event timing of the MC-interval and exchange kernels
+ * issued by gd_remc_run while profiling is on; gd_remc_kernel_times
+ * synchronises, returns the sums since the previous call and resets them. */
+gd_status gd_remc_set_profiling(gd_remc *remc, int on);
+gd_status gd_remc_kernel_times(gd_remc *remc, double *mc_ms, int *mc_launches,
+                               double *exch_ms, int *exch_launches);
+
+/* One call with host buffers: upload, init, steps_total steps, read back,
+ * free.  The counterpart of Run (run.cu:41-353). */
+gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc,
+                 gd_mc_log *log);
+
+/* ------------------------------------------------------------------------ */
+/* Building blocks exposed for testing: the Metropolis and exchange rules   */
+/* on given energies, the counter-based RNG and the decision exp.           */
+/* ------------------------------------------------------------------------ */
+/* accept[i] = u(seed, stream, rep[i], step[i]) < gd_expf(dE[i] * mbeta[i]) */
+gd_status gd_metropolis_dev(gd_ctx *ctx, int n, const float *e_new,
+                            const float *e_old, const float *minus_beta,
+                            const int *rep, const int *step, uint64_t seed,
+                            uint32_t stream_id, int *accept);
+/* Philox4x32-10 blocks and exp evaluated on the device (device pointers). */
+gd_status gd_philox_dev(gd_ctx *ctx, int n, const uint32_t *ctr4,
+                        const uint32_t *key2, uint32_t *out4);
+gd_status gd_expf_dev(gd_ctx *ctx, int n, const float *x, float *y);
+/* FP32 FMA throughput probe (roofline denominator): n_blocks x 256 threads,
+ * 8 chains x 16 FMAs x iters each; returns the time and the flop count. */
+gd_status gd_fma_peak(gd_ctx *ctx, int n_blocks, int iters, float *ms,
+                      double *flops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUDOCK_H */

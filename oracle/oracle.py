@@ -1,0 +1,147 @@
+"""Python wrapper of the CPU oracle (oracle/gd_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline leg, never by the gpudock_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from gpudock_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libgdoracle.so")
+LIB_NATIVE = os.path.join(HERE, "_build", "libgdoracle_native.so")
+
+_libs = {}
+
+
+def build(native: bool = False) -> str:
+    target = "native" if native else "all"
+    path = LIB_NATIVE if native else LIB
+    src = os.path.join(HERE, "gd_oracle.c")
+    if os.path.exists(path) and os.path.getmtime(path) >= os.path.getmtime(src):
+        return path
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    return path
+
+
+def load(native: bool = False):
+    key = "native" if native else "portable"
+    if key in _libs:
+        return _libs[key]
+    path = build(native)
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.orc_philox.argtypes = [P, P, P]
+    lib.orc_expf.argtypes = [C.c_float]
+    lib.orc_expf.restype = C.c_float
+    lib.orc_metropolis.argtypes = [C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_uint32,
+                                   C.c_int, C.c_int]
+    lib.orc_metropolis.restype = C.c_int
+    lib.orc_enepara_optimize.argtypes = [C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara)]
+    lib.orc_set_temperature.argtypes = [C.c_int, C.c_float, C.c_float, P, P]
+    lib.orc_energy_pose.argtypes = [C.POINTER(abi.GdComplex), C.c_int, C.c_int, P, P, P, P]
+    lib.orc_energy_poses.argtypes = [C.POINTER(abi.GdComplex), C.c_int, C.c_int, C.c_int, P, P,
+                                     P, P, C.c_int]
+    lib.orc_exchange.argtypes = [C.POINTER(abi.GdMcParams), C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, P, P, P]
+    lib.orc_remc_run.argtypes = [C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams),
+                                 C.POINTER(abi.GdMcLog), C.c_int]
+    lib.orc_remc_run.restype = C.c_int
+    lib.orc_mc_sample.argtypes = [C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams), C.c_int,
+                                  C.c_int, C.c_int, C.c_int]
+    lib.orc_mc_sample.restype = C.c_longlong
+    lib.orc_max_threads.restype = C.c_int
+    _libs[key] = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def philox(ctr: np.ndarray, key: np.ndarray) -> np.ndarray:
+    lib = load()
+    ctr = np.ascontiguousarray(ctr, np.uint32).reshape(-1, 4)
+    key = np.ascontiguousarray(key, np.uint32).reshape(-1, 2)
+    out = np.zeros_like(ctr)
+    for i in range(ctr.shape[0]):
+        lib.orc_philox(_p(ctr[i]), _p(key[i]), _p(out[i]))
+    return out
+
+
+def expf(x: np.ndarray) -> np.ndarray:
+    lib = load()
+    x = np.asarray(x, np.float32).reshape(-1)
+    return np.array([lib.orc_expf(float(v)) for v in x], np.float32)
+
+
+def metropolis(e_new, e_old, mbeta, seed, stream, rep, step) -> np.ndarray:
+    lib = load()
+    return np.array([lib.orc_metropolis(float(a), float(b), float(m), int(seed), int(stream),
+                                        int(r), int(s))
+                     for a, b, m, r, s in zip(e_new, e_old, mbeta, rep, step)], np.int32)
+
+
+def enepara_optimize(raw: abi.GdEneparaRaw) -> abi.GdEnepara:
+    out = abi.GdEnepara()
+    load().orc_enepara_optimize(C.byref(raw), C.byref(out))
+    return out
+
+
+def set_temperature(n: int, floor_t: float, ceil_t: float):
+    t = np.zeros(n, np.float32)
+    mb = np.zeros(n, np.float32)
+    load().orc_set_temperature(n, floor_t, ceil_t, _p(t), _p(mb))
+    return t, mb
+
+
+def energy_poses(cx: abi.Complex, poses: np.ndarray, prt_conf: int = 0, lig_conf: int = 0,
+                 n_threads: int = 0, native: bool = False):
+    """terms [n,10] f32, raw [n,9] f64, abs_sum [n,5] f64 (|contribution| sums)."""
+    lib = load(native)
+    poses = np.ascontiguousarray(poses, np.float32).reshape(-1, 6)
+    n = poses.shape[0]
+    terms = np.zeros((n, abi.NTERM), np.float32)
+    raw = np.zeros((n, abi.NRAW), np.float64)
+    asum = np.zeros((n, 5), np.float64)
+    lib.orc_energy_poses(C.byref(cx.struct()), prt_conf, lig_conf, n, _p(poses), _p(terms),
+                         _p(raw), _p(asum), n_threads)
+    return terms, raw, asum
+
+
+def exchange(params: abi.GdMcParams, n_prt: int, n_lig: int, n_tmp: int, rnd: int, mode_t: int,
+             etotal: np.ndarray, idx_tmp: np.ndarray):
+    """One exchange round on given totals; returns (new idx_tmp, slot counters)."""
+    et = np.ascontiguousarray(etotal, np.float32)
+    it = np.ascontiguousarray(idx_tmp, np.int32).copy()
+    acs = np.zeros(n_tmp, np.int32)
+    load().orc_exchange(C.byref(params), n_prt, n_lig, n_tmp, rnd, mode_t, _p(et), _p(it),
+                        _p(acs))
+    return it, acs
+
+
+def remc_run(cx: abi.Complex, steps_total: int, steps_per_exchange: int, minus_beta,
+             n_threads: int = 0, **kw) -> abi.McLogBuffers:
+    params, mb = abi.mc_params(steps_total, steps_per_exchange, minus_beta, **kw)
+    n_rep = cx.n_prt * cx.n_lig * len(mb)
+    buf = abi.McLogBuffers(n_rep, len(mb), steps_total, bool(params.flags & abi.MC_RECORD))
+    st = load().orc_remc_run(C.byref(cx.struct()), C.byref(params), C.byref(buf.log), n_threads)
+    if st != 0:
+        raise RuntimeError(f"orc_remc_run: status {st}")
+    return buf
+
+
+def mc_sample(cx: abi.Complex, params: abi.GdMcParams, r0: int, n_rep: int, n_steps: int,
+              n_threads: int = 0, native: bool = False) -> int:
+    return int(load(native).orc_mc_sample(C.byref(cx.struct()), C.byref(params), r0, n_rep,
+                                          n_steps, n_threads))
+
+
+def max_threads(native: bool = False) -> int:
+    return int(load(native).orc_max_threads())
