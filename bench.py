@@ -176,13 +176,18 @@ def run_reference(args):
     threads = orc.max_threads(native)
     params, _keep = abi.mc_params(w.steps, w.steps_per_exchange, mb, w.move_scale, seed=1)
     n_rep_total = cx.n_prt * cx.n_lig * w.n_tmp
-    n_rep = min(n_rep_total, threads * 2)
+    # each step: a replica sample x 2 MC steps sized to about 4 s of CPU work
+    t0 = time.perf_counter()
+    orc.mc_sample(cx, params, 0, threads, 1, threads, native)
+    per_rep_step = max(time.perf_counter() - t0, 1e-4) / threads
+    n_rep = int(min(n_rep_total, max(threads, 4.0 / (2 * per_rep_step))))
     for _ in range(args.warmup):
         orc.mc_sample(cx, params, 0, threads, 1, threads, native)
     t0 = time.perf_counter()
     done = 0
     for k in range(args.steps):
-        done += orc.mc_sample(cx, params, (k * n_rep) % n_rep_total, n_rep, 2, threads, native)
+        done += orc.mc_sample(cx, params, (k * n_rep) % max(1, n_rep_total - n_rep), n_rep, 2,
+                              threads, native)
     dt = time.perf_counter() - t0
     val = done / dt
     line = {
@@ -223,7 +228,10 @@ def main():
     w, cx, mb = build_workload(args.workload, args.seed + 7919 * rank)
     n_rep = cx.n_prt * cx.n_lig * w.n_tmp
     spe = w.steps_per_exchange
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by torch and the library, so the
+    # CUDA events and the L2 flush are ordered with the library's kernels
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = lib.Context(local, stream.cuda_stream)
     dcx = lib.DeviceComplex(ctx, cx)
     total_steps = spe * (args.warmup + args.steps + 2)

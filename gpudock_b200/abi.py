@@ -115,6 +115,10 @@ class GdComplex(C.Structure):
     ]
 
 
+class GdTile(C.Structure):
+    _fields_ = [("atom_groups", C.c_int), ("tile_groups", C.c_int), ("atoms_per_warp", C.c_int)]
+
+
 class GdMcParams(C.Structure):
     _fields_ = [
         ("steps_total", C.c_int), ("steps_per_exchange", C.c_int),

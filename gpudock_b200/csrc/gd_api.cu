@@ -1,11 +1,11 @@
-// gd_api.cu -- host side of the C-ABI in include/gpudock.h: contexts, the
-// device layout of a complex, pose energies, and the REMC run loop.
+// gd_api.cu -- host side of the C-ABI in include/gpudock.h: errors, force
+// field and temperature tables, validation, contexts, the device layout of a
+// complex, pose energies, the launch-shape autotuner and test entry points.
 //
-// Boundary replaced: Run() of gpudocksm-rem-1.2/src/run.cu:41-353 (which
-// staged every table with cudaMemcpy/cudaMemcpyToSymbol, launched
-// MonteCarlo_d / ExchangeReplicas_d synchronously and exit()ed on errors).
-// Here every call returns a status, device memory belongs to handles, and
-// launches are asynchronous on the context stream.
+// Boundary replaced: the table staging of Run() in
+// gpudocksm-rem-1.2/src/run.cu:114-256 (cudaMemcpy / cudaMemcpyToSymbol into
+// __constant__ globals, exit() on any error).  Here every call returns a
+// status and device memory belongs to reference-counted handles.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -19,13 +19,13 @@
 
 #include <cuda_runtime.h>
 
-#include "gd_internal.h"
+#include "gd_common.h"
 
 using namespace gd;
 
-namespace {
+namespace gd {
 
-thread_local std::string g_err;
+static thread_local std::string g_err;
 
 gd_status fail(gd_status st, const char *fmt, ...) {
   char buf[512];
@@ -37,66 +37,108 @@ gd_status fail(gd_status st, const char *fmt, ...) {
   return st;
 }
 
-#define GD_CUDA(call)                                                                  \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess)                                                             \
-      return fail(e_ == cudaErrorMemoryAllocation ? GD_ENOMEM : GD_ECUDA, "%s: %s (%s:%d)", \
-                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                  \
-  } while (0)
+int round_na(int na) {
+  for (int v : kNAValues)
+    if (v >= na) return v;
+  return 0;
+}
 
-#define GD_TRY(call)               \
-  do {                             \
-    gd_status s_ = (call);         \
-    if (s_ != GD_OK) return s_;    \
-  } while (0)
+// Default launch shape: about four atoms per warp (enough independent pair
+// chains to cover the MUFU and FMA latencies), atom groups to cover the
+// ligand, and when the protein is resident as many tile groups as fit in
+// MAX_WARPS.
+Tile default_tile(int lna, bool resident) {
+  Tile t;
+  int na = lna <= 48 ? 4 : (lna <= 72 ? 6 : (lna <= 96 ? 8 : 10));
+  int A = (lna + na - 1) / na;
+  while (A > MAX_WARPS) {
+    na = round_na(na + 1);
+    A = (lna + na - 1) / na;
+  }
+  na = round_na((lna + A - 1) / A);
+  t.A = A;
+  t.NA = na;
+  t.P = resident ? std::max(1, MAX_WARPS / A) : 1;
+  return t;
+}
 
-constexpr float kPI = 3.1415926535f;  // size.h:86
+void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident) {
+  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  const size_t limit = 227 * 1024;
+  if (n_tiles <= MAX_RESIDENT_TILES && dock_smem_bytes(t.A, t.P, t.NA, n_tiles) <= limit) {
+    *n_stages = n_tiles;
+    *resident = 1;
+  } else {
+    *n_stages = STREAM_STAGES;
+    *resident = 0;
+  }
+}
 
-}  // namespace
+static bool fits_resident(const KTables &T, const Tile &t) {
+  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  return n_tiles <= MAX_RESIDENT_TILES &&
+         dock_smem_bytes(t.A, t.P, t.NA, n_tiles) <= 227 * 1024;
+}
 
-// ---------------------------------------------------------------------------
-// Opaque handles
-// ---------------------------------------------------------------------------
-struct gd_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int *d_err = nullptr;
-  uint64_t launches = 0;
-  int n_sm = 148;
-};
+Tile tile_for(gd_ctx *ctx, const KTables &T) {
+  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  {
+    std::lock_guard<std::mutex> g(ctx->tile_mu);
+    auto it = ctx->tiles.find({T.lna, n_tiles});
+    if (it != ctx->tiles.end()) return it->second;
+  }
+  Tile t = default_tile(T.lna, true);
+  if (!fits_resident(T, t)) t = default_tile(T.lna, false);
+  return t;
+}
 
-struct gd_dcomplex {
-  gd_ctx *ctx = nullptr;
-  KTables T{};
-  std::vector<void *> allocs;
-  size_t bytes = 0;
-};
+void ctx_retain(gd_ctx *c) {
+  if (c) c->refs++;
+}
 
-struct gd_remc {
-  gd_ctx *ctx = nullptr;
-  const gd_dcomplex *dcx = nullptr;
-  gd_mc_params mc{};
-  std::vector<float> minus_beta;
-  KState st{};
-  int n_prt = 0, n_lig = 0, n_tmp = 0, n_rep = 0;
-  int *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
-  int n_cta = 0;
-  int step = 0;  // MC steps done since init
-  int n_warps = 0, n_stages = 0, resident = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  bool timing = false;
-  double t_compute = 0.0;
-  std::vector<void *> allocs;
-  // optional per-launch timing of the MC and exchange kernels
-  bool profile = false;
-  std::vector<cudaEvent_t> prof_ev;  // pairs: start, stop
-  std::vector<int> prof_kind;        // 0 = MC interval, 1 = exchange
-};
+void ctx_release(gd_ctx *c) {
+  if (!c || --c->refs > 0) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_err);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
 
-extern "C" const char *gd_last_error(void) { return g_err.c_str(); }
-extern "C" const char *gd_version(void) { return "gpudock-b200 0.1 (sm_100a)"; }
+void dcx_retain(gd_dcomplex *d) {
+  if (d) d->refs++;
+}
+
+void dcx_release(gd_dcomplex *d) {
+  if (!d || --d->refs > 0) return;
+  if (d->ctx) {
+    cudaSetDevice(d->ctx->device);
+    cudaStreamSynchronize(d->ctx->stream);
+  }
+  for (void *p : d->allocs) cudaFree(p);
+  gd_ctx *c = d->ctx;
+  gd_dcomplex *owner = d->protein_owner;
+  delete d;
+  dcx_release(owner);
+  ctx_release(c);
+}
+
+gd_status ctx_check(gd_ctx *c) {
+  int h = 0;
+  GD_CUDA(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  GD_CUDA(cudaStreamSynchronize(c->stream));
+  if (h != 0) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+    cudaStreamSynchronize(c->stream);
+    return fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)", h);
+  }
+  return GD_OK;
+}
+
+}  // namespace gd
+
+extern "C" const char *gd_last_error(void) { return gd::g_err.c_str(); }
+extern "C" const char *gd_version(void) { return "gpudock-b200 0.2 (sm_100a)"; }
 
 // ---------------------------------------------------------------------------
 // Force-field tables (OptimizeEnepara, util.C:405-458) and temperatures
@@ -174,8 +216,9 @@ extern "C" gd_status gd_complex_validate(const gd_complex *cx) {
   const gd_ligand &L = cx->lig;
   const gd_protein &P = cx->prt;
   if (!cx->ff) return fail(GD_EINVAL, "force field is NULL");
-  if (L.lna < 1 || L.lna > MAX_WARPS * MAX_APW)
-    return fail(GD_EINVAL, "ligand atoms lna=%d outside [1, %d]", L.lna, MAX_WARPS * MAX_APW);
+  if (L.lna < 1 || L.lna > MAX_WARPS * MAX_NA || L.lna > MAX_LNA)
+    return fail(GD_EINVAL, "ligand atoms lna=%d outside [1, %d]", L.lna,
+                std::min(MAX_WARPS * MAX_NA, MAX_LNA));
   if (L.n_conf < 1) return fail(GD_EINVAL, "ligand conformations n_conf=%d", L.n_conf);
   if (!L.x || !L.y || !L.z || !L.t || !L.c || !L.n) return fail(GD_EINVAL, "ligand array NULL");
   if (P.pnp < 1 || P.n_conf < 1)
@@ -254,24 +297,7 @@ extern "C" gd_status gd_ctx_create(int device, void *stream, gd_ctx **out) {
 }
 
 extern "C" gd_status gd_ctx_destroy(gd_ctx *c) {
-  if (!c) return GD_OK;
-  cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
-  cudaFree(c->d_err);
-  if (c->own_stream) cudaStreamDestroy(c->stream);
-  delete c;
-  return GD_OK;
-}
-
-static gd_status ctx_check(gd_ctx *c) {
-  int h = 0;
-  GD_CUDA(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  GD_CUDA(cudaStreamSynchronize(c->stream));
-  if (h != 0) {
-    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
-    cudaStreamSynchronize(c->stream);
-    return fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)", h);
-  }
+  ctx_release(c);
   return GD_OK;
 }
 
@@ -301,27 +327,17 @@ static gd_status upload(gd_dcomplex *d, const std::vector<T> &h, const T **out) 
 }
 
 extern "C" gd_status gd_complex_free(gd_dcomplex *d) {
-  if (!d) return GD_OK;
-  if (d->ctx) {
-    cudaSetDevice(d->ctx->device);
-    cudaStreamSynchronize(d->ctx->stream);
-  }
-  for (void *p : d->allocs) cudaFree(p);
-  delete d;
+  dcx_release(d);
   return GD_OK;
 }
 
 extern "C" size_t gd_complex_device_bytes(const gd_dcomplex *d) { return d ? d->bytes : 0; }
 
-static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomplex *d) {
-  const gd_ligand &L = cx->lig;
-  const gd_protein &P = cx->prt;
-  const gd_enepara &F = *cx->ff;
+// Packs the protein conformations into {x, y, z, ele} and {hpp, meta}.
+static gd_status upload_protein(const gd_protein &P, gd_dcomplex *d) {
   KTables &T = d->T;
-  const int lna = L.lna, pnp = P.pnp;
+  const int pnp = P.pnp;
   const int pnp_pad = (pnp + TILE_PTS - 1) / TILE_PTS * TILE_PTS;
-
-  // protein points: {x, y, z, ele} per conformation, {hpp, meta} shared
   std::vector<float4> pa((size_t)P.n_conf * pnp_pad, make_float4(0.f, 0.f, 0.f, 0.f));
   for (int c = 0; c < P.n_conf; ++c)
     for (int p = 0; p < pnp; ++p) {
@@ -337,15 +353,31 @@ static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomp
     std::memcpy(&mf, &meta, 4);
     pb[p] = make_float2(P.hpp[p], mf);
   }
-  // type-pair table [lig type][point type]
-  std::vector<float4> ta(GD_NLT * GD_NPT);
-  std::vector<float2> tb(GD_NLT * GD_NPT);
+  GD_TRY(upload(d, pa, &T.pt_a));
+  GD_TRY(upload(d, pb, &T.pt_b));
+  T.pnp = pnp;
+  T.pnp_pad = pnp_pad;
+  T.n_prt = P.n_conf;
+  return GD_OK;
+}
+
+// Ligand, pocket template and force-field tables of a complex.
+static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
+  const gd_ligand &L = cx->lig;
+  const gd_enepara &F = *cx->ff;
+  KTables &T = d->T;
+  const int lna = L.lna;
+  // type-pair table [lig type][point type], plus an all-zero row for the
+  // padding atoms of the last atom group
+  std::vector<float4> ta(TAB_ROWS * GD_NPT, make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<float2> tb(TAB_ROWS * GD_NPT, make_float2(0.f, 0.f));
+  float max_pmf0 = 0.f;
   for (int i = 0; i < GD_NLT; ++i)
     for (int j = 0; j < GD_NPT; ++j) {
       ta[i * GD_NPT + j] = make_float4(F.p1a[i][j], F.p2a[i][j], F.pmf0[i][j], F.pmf1[i][j]);
       tb[i * GD_NPT + j] = make_float2(F.hdb0[i][j], F.hdb1[i][j]);
+      max_pmf0 = std::max(max_pmf0, F.pmf0[i][j]);
     }
-  // ligand conformations
   std::vector<float4> lg((size_t)L.n_conf * lna);
   for (size_t i = 0; i < lg.size(); ++i) lg[i] = make_float4(L.x[i], L.y[i], L.z[i], 0.f);
   std::vector<int> lt(L.t, L.t + lna);
@@ -377,9 +409,6 @@ static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomp
     tcc[m] = cx->mcs.tcc[m];
     cnt[m] = (float)c;
   }
-
-  GD_TRY(upload(d, pa, &T.pt_a));
-  GD_TRY(upload(d, pb, &T.pt_b));
   GD_TRY(upload(d, ta, &T.tab_a));
   GD_TRY(upload(d, tb, &T.tab_b));
   GD_TRY(upload(d, lg, &T.lig));
@@ -394,9 +423,6 @@ static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomp
 
   T.lna = lna;
   T.n_lig = L.n_conf;
-  T.pnp = pnp;
-  T.pnp_pad = pnp_pad;
-  T.n_prt = P.n_conf;
   T.pos = pos;
   T.psp_ncol = cx->psp.n_col;
   T.lj0 = F.lj0;
@@ -409,6 +435,11 @@ static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomp
   T.kde2 = F.kde2;
   T.kde3 = F.kde3;
   T.s2pi = sqrtf(2.0f * kPI);
+  // every close-range term fires inside this squared distance: hydrophobic
+  // d^2 <= 81, near-field electrostatics el1 d < 1, psp d <= pmf0
+  const float r_ele = F.el1 > 0.f ? 1.0f / F.el1 : 1e30f;
+  const float r_max = std::max(9.0f, std::max(r_ele, max_pmf0));
+  T.near_d2 = r_max * r_max * 1.0001f + 1e-3f;
   for (int i = 0; i < GD_NLT; ++i) {
     T.hpl0[i] = F.hpl0[i];
     T.hpl1[i] = F.hpl1[i];
@@ -421,59 +452,103 @@ static gd_status complex_upload_impl(gd_ctx *ctx, const gd_complex *cx, gd_dcomp
   }
   for (int i = 0; i < 3; ++i) {
     T.lig_center[i] = L.center[i];
-    T.pocket[i] = P.pocket_center[i];
+    T.pocket[i] = cx->prt.pocket_center[i];
   }
-  GD_CUDA(cudaStreamSynchronize(ctx->stream));
   return GD_OK;
 }
 
-extern "C" gd_status gd_complex_upload(gd_ctx *ctx, const gd_complex *cx, gd_dcomplex **out) {
+static gd_status complex_upload_common(gd_ctx *ctx, const gd_complex *cx,
+                                       const gd_dcomplex *share, int prt_conf0, int n_prt,
+                                       gd_dcomplex **out) {
   if (!ctx || !out) return fail(GD_EINVAL, "gd_complex_upload: NULL argument");
   *out = nullptr;
   GD_TRY(gd_complex_validate(cx));
+  if (share) {
+    if (share->ctx != ctx) return fail(GD_EINVAL, "shared protein belongs to another context");
+    if (share->T.pnp != cx->prt.pnp)
+      return fail(GD_EINVAL, "shared protein has %d points, complex %d", share->T.pnp,
+                  cx->prt.pnp);
+    if (prt_conf0 < 0 || n_prt < 1 || prt_conf0 + n_prt > share->T.n_prt)
+      return fail(GD_EINVAL, "conformations [%d, %d) outside the shared protein's %d", prt_conf0,
+                  prt_conf0 + n_prt, share->T.n_prt);
+  }
   GD_CUDA(cudaSetDevice(ctx->device));
   gd_dcomplex *d = new (std::nothrow) gd_dcomplex;
   if (!d) return fail(GD_ENOMEM, "host allocation");
   d->ctx = ctx;
-  gd_status st;
+  ctx_retain(ctx);
+  gd_status st = GD_OK;
   try {
-    st = complex_upload_impl(ctx, cx, d);
+    if (share) {
+      d->protein_owner = const_cast<gd_dcomplex *>(share);
+      dcx_retain(d->protein_owner);
+      d->T.pt_a = share->T.pt_a + (size_t)prt_conf0 * share->T.pnp_pad;
+      d->T.pt_b = share->T.pt_b;
+      d->T.pnp = share->T.pnp;
+      d->T.pnp_pad = share->T.pnp_pad;
+      d->T.n_prt = n_prt;
+    } else {
+      st = upload_protein(cx->prt, d);
+    }
+    if (st == GD_OK) st = upload_ligand(cx, d);
+    if (st == GD_OK) {
+      cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) st = fail(GD_ECUDA, "upload: %s", cudaGetErrorString(e));
+    }
   } catch (const std::bad_alloc &) {
     st = fail(GD_ENOMEM, "host allocation while packing the complex");
   }
   if (st != GD_OK) {
-    gd_complex_free(d);
+    dcx_release(d);
     return st;
   }
   *out = d;
   return GD_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Launch shape
-// ---------------------------------------------------------------------------
-static int pick_warps(int lna) {
-  int w = (lna + 2) / 3;  // about three ligand atoms per warp
-  w = std::max(4, std::min(MAX_WARPS, w));
-  while (w * MAX_APW < lna) ++w;
-  return w;
+extern "C" gd_status gd_complex_upload(gd_ctx *ctx, const gd_complex *cx, gd_dcomplex **out) {
+  return complex_upload_common(ctx, cx, nullptr, 0, 0, out);
 }
 
-static void pick_stages(const KTables &T, int n_warps, int *n_stages, int *resident) {
-  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
-  const size_t limit = 227 * 1024;
-  if (n_tiles <= MAX_RESIDENT_TILES && dock_smem_bytes(n_warps, n_tiles) <= limit) {
-    *n_stages = n_tiles;
-    *resident = 1;
-  } else {
-    *n_stages = STREAM_STAGES;
-    *resident = 0;
-  }
+extern "C" gd_status gd_complex_upload_shared(gd_ctx *ctx, const gd_complex *cx,
+                                              const gd_dcomplex *protein, int prt_conf0,
+                                              int n_prt, gd_dcomplex **out) {
+  if (!protein) return fail(GD_EINVAL, "gd_complex_upload_shared: protein is NULL");
+  return complex_upload_common(ctx, cx, protein, prt_conf0, n_prt, out);
 }
 
 // ---------------------------------------------------------------------------
 // Pose energies
 // ---------------------------------------------------------------------------
+static gd_status poses_launch(gd_ctx *ctx, const gd_dcomplex *d, const Tile &tile, int prt_conf,
+                              int lig_conf, int n_pose, const float *poses, float *terms,
+                              double *raw, KItem **d_item) {
+  KRun R{};
+  R.mode = KMODE_POSES;
+  R.A = tile.A;
+  R.P = tile.P;
+  pick_stages(d->T, tile, &R.n_stages, &R.resident);
+  if (!R.resident) R.P = 1;
+  R.prt_conf = prt_conf;
+  R.lig_conf = lig_conf;
+  R.n_pose = n_pose;
+  R.poses = poses;
+  R.terms = terms;
+  R.raw = raw;
+  R.err = ctx->d_err;
+  KItem it{};
+  it.T = d->T;
+  it.n_tmp = 1;
+  it.n_lig_conf = d->T.n_lig;
+  it.n_prt = d->T.n_prt;
+  GD_CUDA(cudaMallocAsync((void **)d_item, sizeof(KItem), ctx->stream));
+  GD_CUDA(cudaMemcpyAsync(*d_item, &it, sizeof(KItem), cudaMemcpyHostToDevice, ctx->stream));
+  R.items = *d_item;
+  GD_CUDA(launch_dock(R, tile.NA, (n_pose + 31) / 32, ctx->stream));
+  ctx->launches += 1;
+  return GD_OK;
+}
+
 extern "C" gd_status gd_energy_poses_dev(gd_ctx *ctx, const gd_dcomplex *d, int prt_conf,
                                          int lig_conf, int n_pose, const float *poses,
                                          float *terms, double *raw) {
@@ -485,21 +560,12 @@ extern "C" gd_status gd_energy_poses_dev(gd_ctx *ctx, const gd_dcomplex *d, int 
     return fail(GD_EINVAL, "lig_conf %d outside [0, %d)", lig_conf, d->T.n_lig);
   if (n_pose == 0) return GD_OK;
   if (!poses || !terms) return fail(GD_EINVAL, "poses/terms NULL");
-  KRun R{};
-  R.mode = KMODE_POSES;
-  R.n_warps = pick_warps(d->T.lna);
-  pick_stages(d->T, R.n_warps, &R.n_stages, &R.resident);
-  R.prt_conf = prt_conf;
-  R.lig_conf = lig_conf;
-  R.n_pose = n_pose;
-  R.poses = poses;
-  R.terms = terms;
-  R.raw = raw;
-  R.err = ctx->d_err;
   GD_CUDA(cudaSetDevice(ctx->device));
-  GD_CUDA(launch_dock(d->T, R, (n_pose + 31) / 32, ctx->stream));
-  ctx->launches += 1;
-  return GD_OK;
+  KItem *dit = nullptr;
+  gd_status st = poses_launch(ctx, d, tile_for(ctx, d->T), prt_conf, lig_conf, n_pose, poses,
+                              terms, raw, &dit);
+  if (dit) cudaFreeAsync(dit, ctx->stream);
+  return st;
 }
 
 extern "C" gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *d, int prt_conf,
@@ -545,291 +611,96 @@ extern "C" gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *d, int prt_
 }
 
 // ---------------------------------------------------------------------------
-// REMC
+// Launch-shape autotuner: times the energy kernel on one wave of CTAs of
+// random poses for every compiled shape that covers the ligand and keeps the
+// fastest; the choice is cached in the context per (ligand atoms, protein
+// tiles) and used by every later launch for that size class.
 // ---------------------------------------------------------------------------
-extern "C" int gd_remc_n_rep(const gd_remc *r) { return r ? r->n_rep : 0; }
-
-extern "C" gd_status gd_remc_destroy(gd_remc *r) {
-  if (!r) return GD_OK;
-  if (r->ctx) {
-    cudaSetDevice(r->ctx->device);
-    cudaStreamSynchronize(r->ctx->stream);
-  }
-  for (void *p : r->allocs) cudaFree(p);
-  for (cudaEvent_t e : r->prof_ev) cudaEventDestroy(e);
-  if (r->ev0) cudaEventDestroy(r->ev0);
-  if (r->ev1) cudaEventDestroy(r->ev1);
-  delete r;
-  return GD_OK;
-}
-
-template <typename T>
-static gd_status dalloc(gd_remc *r, T **out, size_t n) {
-  void *p = nullptr;
-  GD_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
-  r->allocs.push_back(p);
-  GD_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), r->ctx->stream));
-  *out = (T *)p;
-  return GD_OK;
-}
-
-static gd_status validate_mc(const gd_mc_params *mc) {
-  if (!mc) return fail(GD_EINVAL, "mc params NULL");
-  if (mc->n_tmp < 1 || mc->n_tmp > MAX_TMP)
-    return fail(GD_EINVAL, "n_tmp=%d outside [1, %d]", mc->n_tmp, MAX_TMP);
-  if (!mc->minus_beta) return fail(GD_EINVAL, "minus_beta NULL");
-  if (mc->steps_total < 0) return fail(GD_EINVAL, "steps_total=%d", mc->steps_total);
-  if (mc->steps_per_exchange < 1)
-    return fail(GD_EINVAL, "steps_per_exchange=%d", mc->steps_per_exchange);
-  if (mc->steps_total % mc->steps_per_exchange != 0)
-    return fail(GD_EINVAL, "steps_total %d is not a multiple of steps_per_exchange %d",
-                mc->steps_total, mc->steps_per_exchange);
-  for (int i = 0; i < mc->n_tmp; ++i)
-    if (!std::isfinite(mc->minus_beta[i])) return fail(GD_EINVAL, "minus_beta[%d] not finite", i);
-  return GD_OK;
-}
-
-static gd_status remc_create_impl(gd_ctx *ctx, const gd_dcomplex *d, const gd_mc_params *mc,
-                                  gd_remc *r) {
-  r->ctx = ctx;
-  r->dcx = d;
-  r->mc = *mc;
-  r->minus_beta.assign(mc->minus_beta, mc->minus_beta + mc->n_tmp);
-  r->mc.minus_beta = r->minus_beta.data();
-  r->n_prt = d->T.n_prt;
-  r->n_lig = d->T.n_lig;
-  r->n_tmp = mc->n_tmp;
-  const long long nrep = (long long)r->n_prt * r->n_lig * r->n_tmp;
-  if (nrep > (1LL << 30)) return fail(GD_EINVAL, "too many replicas: %lld", nrep);
-  r->n_rep = (int)nrep;
-  KState &S = r->st;
-  GD_TRY(dalloc(r, &S.m_old, (size_t)r->n_rep * 6));
-  GD_TRY(dalloc(r, &S.e_old, (size_t)r->n_rep * GD_NTERM));
-  GD_TRY(dalloc(r, &S.idx_tmp, (size_t)r->n_rep));
-  GD_TRY(dalloc(r, &S.acs_mc, (size_t)r->n_rep));
-  GD_TRY(dalloc(r, &S.acs_exchg, (size_t)r->n_tmp));
-  float *mb = nullptr;
-  GD_TRY(dalloc(r, &mb, (size_t)r->n_tmp));
-  GD_CUDA(cudaMemcpyAsync(mb, r->minus_beta.data(), sizeof(float) * r->n_tmp,
-                          cudaMemcpyHostToDevice, ctx->stream));
-  S.minus_beta = mb;
-  S.n_rep = r->n_rep;
-  S.n_tmp = r->n_tmp;
-  S.n_lig_conf = r->n_lig;
-  S.record = nullptr;
-  S.rec_steps = 0;
-  if (mc->flags & GD_MC_RECORD) {
-    gd_record *rec = nullptr;
-    GD_TRY(dalloc(r, &rec, (size_t)r->n_rep * std::max(1, mc->steps_total)));
-    S.record = rec;
-    S.rec_steps = mc->steps_total;
-  }
-  // CTAs: up to 32 consecutive replicas of the same protein conformation
-  std::vector<int> c0, cn;
-  const int per_p = r->n_tmp * r->n_lig;
-  for (int p = 0; p < r->n_prt; ++p)
-    for (int j = 0; j < per_p; j += 32) {
-      c0.push_back(p * per_p + j);
-      cn.push_back(std::min(32, per_p - j));
-    }
-  r->n_cta = (int)c0.size();
-  GD_TRY(dalloc(r, &r->d_cta_rep0, c0.size()));
-  GD_TRY(dalloc(r, &r->d_cta_nrep, cn.size()));
-  GD_CUDA(cudaMemcpyAsync(r->d_cta_rep0, c0.data(), sizeof(int) * c0.size(),
-                          cudaMemcpyHostToDevice, ctx->stream));
-  GD_CUDA(cudaMemcpyAsync(r->d_cta_nrep, cn.data(), sizeof(int) * cn.size(),
-                          cudaMemcpyHostToDevice, ctx->stream));
-  r->n_warps = pick_warps(d->T.lna);
-  pick_stages(d->T, r->n_warps, &r->n_stages, &r->resident);
-  GD_CUDA(cudaEventCreate(&r->ev0));
-  GD_CUDA(cudaEventCreate(&r->ev1));
-  GD_CUDA(cudaStreamSynchronize(ctx->stream));
-  return GD_OK;
-}
-
-extern "C" gd_status gd_remc_create(gd_ctx *ctx, const gd_dcomplex *d, const gd_mc_params *mc,
-                                    gd_remc **out) {
-  if (!ctx || !d || !out) return fail(GD_EINVAL, "gd_remc_create: NULL argument");
-  *out = nullptr;
-  GD_TRY(validate_mc(mc));
+extern "C" gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *d, gd_tile *best,
+                                 double *best_ms) {
+  if (!ctx || !d) return fail(GD_EINVAL, "gd_autotune: NULL handle");
   GD_CUDA(cudaSetDevice(ctx->device));
-  gd_remc *r = new (std::nothrow) gd_remc;
-  if (!r) return fail(GD_ENOMEM, "host allocation");
-  gd_status st;
-  try {
-    st = remc_create_impl(ctx, d, mc, r);
-  } catch (const std::bad_alloc &) {
-    st = fail(GD_ENOMEM, "host allocation");
+  const int lna = d->T.lna;
+  const int n_pose = 32 * ctx->n_sm;
+  std::vector<float> hp((size_t)n_pose * 6);
+  uint32_t s = 12345u;
+  for (auto &v : hp) {
+    s = s * 1664525u + 1013904223u;
+    v = ((s >> 8) * 0x1p-24f - 0.5f) * 2.0f;  // within +-1 A / +-1 rad
   }
-  if (st != GD_OK) {
-    gd_remc_destroy(r);
-    return st;
-  }
-  *out = r;
-  return GD_OK;
-}
-
-static KRun remc_run_desc(const gd_remc *r, int mode) {
-  KRun R{};
-  R.mode = mode;
-  R.n_warps = r->n_warps;
-  R.n_stages = r->n_stages;
-  R.resident = r->resident;
-  R.cta_rep0 = r->d_cta_rep0;
-  R.cta_nrep = r->d_cta_nrep;
-  for (int i = 0; i < 6; ++i) R.move_scale[i] = r->mc.move_scale[i];
-  R.seed = r->mc.seed;
-  R.stream_id = r->mc.stream_id;
-  R.flags = r->mc.flags;
-  R.st = r->st;
-  R.err = r->ctx->d_err;
-  return R;
-}
-
-extern "C" gd_status gd_remc_init(gd_remc *r) {
-  if (!r) return fail(GD_EINVAL, "remc NULL");
-  GD_CUDA(cudaSetDevice(r->ctx->device));
-  KRun R = remc_run_desc(r, KMODE_INIT);
-  R.step0 = 0;
-  R.n_steps = 1;
-  GD_CUDA(cudaMemsetAsync(r->st.acs_exchg, 0, sizeof(int) * r->n_tmp, r->ctx->stream));
-  GD_CUDA(launch_dock(r->dcx->T, R, r->n_cta, r->ctx->stream));
-  r->ctx->launches += 1;
-  r->step = 0;
-  r->t_compute = 0.0;
-  return GD_OK;
-}
-
-extern "C" gd_status gd_remc_run(gd_remc *r, int n_steps) {
-  if (!r) return fail(GD_EINVAL, "remc NULL");
-  const int spe = r->mc.steps_per_exchange;
-  if (n_steps < 0 || n_steps % spe != 0)
-    return fail(GD_EINVAL, "n_steps %d is not a multiple of steps_per_exchange %d", n_steps, spe);
-  if (n_steps == 0) return GD_OK;
-  GD_CUDA(cudaSetDevice(r->ctx->device));
-  GD_CUDA(cudaEventRecord(r->ev0, r->ctx->stream));
-  KRun R = remc_run_desc(r, KMODE_REMC);
-  auto mark = [&](int kind) -> cudaError_t {
-    cudaEvent_t e;
-    cudaError_t st = cudaEventCreate(&e);
-    if (st != cudaSuccess) return st;
-    r->prof_ev.push_back(e);
-    r->prof_kind.push_back(kind);
-    return cudaEventRecord(e, r->ctx->stream);
-  };
-  for (int s0 = r->step; s0 < r->step + n_steps; s0 += spe) {
-    R.step0 = s0;
-    R.n_steps = spe;
-    if (r->profile) GD_CUDA(mark(0));
-    GD_CUDA(launch_dock(r->dcx->T, R, r->n_cta, r->ctx->stream));
-    if (r->profile) GD_CUDA(mark(0));
-    r->ctx->launches += 1;
-    if (r->mc.flags & GD_MC_EXCHANGE) {
-      const int dump = r->mc.steps_per_dump;
-      const int within = dump > 0 ? (s0 % dump) : s0;
-      const int mode_t = (within / spe) % 2;
-      if (r->profile) GD_CUDA(mark(1));
-      GD_CUDA(launch_exchange(r->st, r->n_prt, r->n_lig, r->mc.seed, r->mc.stream_id, s0 / spe,
-                              mode_t, r->ctx->stream));
-      if (r->profile) GD_CUDA(mark(1));
-      r->ctx->launches += 1;
+  float *dp = nullptr, *dt = nullptr;
+  GD_CUDA(cudaMalloc(&dp, hp.size() * sizeof(float)));
+  GD_CUDA(cudaMalloc(&dt, (size_t)n_pose * GD_NTERM * sizeof(float)));
+  GD_CUDA(cudaMemcpy(dp, hp.data(), hp.size() * sizeof(float), cudaMemcpyHostToDevice));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  Tile best_t;
+  float best_time = 1e30f;
+  gd_status st = GD_OK;
+  for (int na : kNAValues) {
+    const int A = (lna + na - 1) / na;
+    if (A > MAX_WARPS || (A > 1 && round_na((lna + A - 1) / A) != na)) continue;
+    for (int P = 1; A * P <= MAX_WARPS; ++P) {
+      Tile t;
+      t.A = A;
+      t.P = P;
+      t.NA = na;
+      if (A * P < 4 && A * P * 2 <= MAX_WARPS) continue;  // too few warps per SM
+      int ns, res;
+      pick_stages(d->T, t, &ns, &res);
+      if (!res && P > 1) continue;
+      float ms_min = 1e30f;
+      for (int rep = 0; rep < 3 && st == GD_OK; ++rep) {
+        KItem *dit = nullptr;
+        cudaEventRecord(e0, ctx->stream);
+        st = poses_launch(ctx, d, t, 0, 0, n_pose, dp, dt, nullptr, &dit);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        if (dit) cudaFree(dit);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) ms_min = std::min(ms_min, ms);
+      }
+      if (st != GD_OK) break;
+      if (ms_min < best_time) {
+        best_time = ms_min;
+        best_t = t;
+      }
     }
   }
-  GD_CUDA(cudaEventRecord(r->ev1, r->ctx->stream));
-  r->timing = true;
-  r->step += n_steps;
-  return GD_OK;
-}
-
-extern "C" gd_status gd_remc_read(gd_remc *r, gd_mc_log *log) {
-  if (!r || !log) return fail(GD_EINVAL, "gd_remc_read: NULL argument");
-  GD_CUDA(cudaSetDevice(r->ctx->device));
-  GD_TRY(ctx_check(r->ctx));
-  if (r->timing) {
-    float ms = 0.f;
-    GD_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
-    r->t_compute += ms * 1e-3;
-    r->timing = false;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dp);
+  cudaFree(dt);
+  GD_TRY(st);
+  GD_TRY(ctx_check(ctx));
+  if (!best_t.valid()) return fail(GD_EINVAL, "no launch shape fits lna=%d", lna);
+  {
+    std::lock_guard<std::mutex> g(ctx->tile_mu);
+    ctx->tiles[{lna, (d->T.pnp + TILE_PTS - 1) / TILE_PTS}] = best_t;
   }
-  const size_t n = (size_t)r->n_rep;
-  std::vector<int> acs(n), acx(r->n_tmp);
-  cudaStream_t s = r->ctx->stream;
-  GD_CUDA(cudaMemcpyAsync(acs.data(), r->st.acs_mc, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-  GD_CUDA(cudaMemcpyAsync(acx.data(), r->st.acs_exchg, sizeof(int) * r->n_tmp,
-                          cudaMemcpyDeviceToHost, s));
-  if (log->energy)
-    GD_CUDA(cudaMemcpyAsync(log->energy, r->st.e_old, sizeof(float) * GD_NTERM * n,
-                            cudaMemcpyDeviceToHost, s));
-  if (log->movematrix)
-    GD_CUDA(cudaMemcpyAsync(log->movematrix, r->st.m_old, sizeof(float) * 6 * n,
-                            cudaMemcpyDeviceToHost, s));
-  if (log->idx_tmp)
-    GD_CUDA(cudaMemcpyAsync(log->idx_tmp, r->st.idx_tmp, sizeof(int) * n, cudaMemcpyDeviceToHost,
-                            s));
-  if (log->record && r->st.record)
-    GD_CUDA(cudaMemcpyAsync(log->record, r->st.record,
-                            sizeof(gd_record) * n * std::max(1, r->st.rec_steps),
-                            cudaMemcpyDeviceToHost, s));
-  GD_CUDA(cudaStreamSynchronize(s));
-  log->ac_mc = 0;
-  for (size_t i = 0; i < n; ++i) log->ac_mc += acs[i];
-  log->ac_temp_exchg = 0;
-  for (int t = 0; t < r->n_tmp; ++t) log->ac_temp_exchg += acx[t];
-  if (log->acs_mc) std::memcpy(log->acs_mc, acs.data(), sizeof(int) * n);
-  if (log->acs_temp_exchg) std::memcpy(log->acs_temp_exchg, acx.data(), sizeof(int) * r->n_tmp);
-  log->t_compute = r->t_compute;
-  return GD_OK;
-}
-
-extern "C" gd_status gd_remc_set_profiling(gd_remc *r, int on) {
-  if (!r) return fail(GD_EINVAL, "remc NULL");
-  r->profile = on != 0;
-  return GD_OK;
-}
-
-extern "C" gd_status gd_remc_kernel_times(gd_remc *r, double *mc_ms, int *mc_launches,
-                                          double *exch_ms, int *exch_launches) {
-  if (!r || !mc_ms || !mc_launches || !exch_ms || !exch_launches)
-    return fail(GD_EINVAL, "gd_remc_kernel_times: NULL argument");
-  GD_CUDA(cudaSetDevice(r->ctx->device));
-  GD_CUDA(cudaStreamSynchronize(r->ctx->stream));
-  *mc_ms = *exch_ms = 0.0;
-  *mc_launches = *exch_launches = 0;
-  for (size_t i = 0; i + 1 < r->prof_ev.size(); i += 2) {
-    float ms = 0.f;
-    GD_CUDA(cudaEventElapsedTime(&ms, r->prof_ev[i], r->prof_ev[i + 1]));
-    if (r->prof_kind[i] == 0) {
-      *mc_ms += ms;
-      *mc_launches += 1;
-    } else {
-      *exch_ms += ms;
-      *exch_launches += 1;
-    }
+  if (best) {
+    best->atom_groups = best_t.A;
+    best->tile_groups = best_t.P;
+    best->atoms_per_warp = best_t.NA;
   }
-  for (cudaEvent_t e : r->prof_ev) cudaEventDestroy(e);
-  r->prof_ev.clear();
-  r->prof_kind.clear();
+  if (best_ms) *best_ms = best_time;
   return GD_OK;
 }
 
-extern "C" gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log) {
-  const auto t0 = std::chrono::steady_clock::now();
-  GD_TRY(validate_mc(mc));
-  gd_ctx *ctx = nullptr;
-  GD_TRY(gd_ctx_create(0, nullptr, &ctx));
-  gd_dcomplex *d = nullptr;
-  gd_remc *r = nullptr;
-  gd_status st = gd_complex_upload(ctx, cx, &d);
-  if (st == GD_OK) st = gd_remc_create(ctx, d, mc, &r);
-  if (st == GD_OK) st = gd_remc_init(r);
-  if (st == GD_OK) st = gd_remc_run(r, mc->steps_total);
-  if (st == GD_OK && log) st = gd_remc_read(r, log);
-  gd_remc_destroy(r);
-  gd_complex_free(d);
-  gd_ctx_destroy(ctx);
-  if (st == GD_OK && log)
-    log->t_wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return st;
+extern "C" gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile) {
+  if (!ctx || !tile) return fail(GD_EINVAL, "gd_ctx_set_tile: NULL argument");
+  Tile t;
+  t.A = tile->atom_groups;
+  t.P = tile->tile_groups;
+  t.NA = tile->atoms_per_warp;
+  if (!t.valid() || t.A * t.P > MAX_WARPS || round_na(t.NA) != t.NA || t.A * t.NA < lna)
+    return fail(GD_EINVAL, "tile %dx%d with %d atoms per warp does not cover %d atoms", t.A, t.P,
+                t.NA, lna);
+  std::lock_guard<std::mutex> g(ctx->tile_mu);
+  ctx->tiles[{lna, (pnp + TILE_PTS - 1) / TILE_PTS}] = t;
+  return GD_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -866,8 +737,6 @@ extern "C" gd_status gd_expf_dev(gd_ctx *ctx, int n, const float *x, float *y) {
   return GD_OK;
 }
 
-// FP32 FMA throughput probe for the roofline denominator (not in the public
-// header's main API; exported for the bench).
 extern "C" gd_status gd_fma_peak(gd_ctx *ctx, int n_blocks, int iters, float *ms_out,
                                  double *flops_out) {
   if (!ctx || n_blocks < 1 || iters < 1 || !ms_out || !flops_out)

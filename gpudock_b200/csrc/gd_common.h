@@ -1,0 +1,86 @@
+// gd_common.h -- host-side internals shared by gd_api.cu and gd_ensemble.cu:
+// the opaque handle types, error reporting and launch-shape selection.
+#pragma once
+
+#include <atomic>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gd_internal.h"
+
+namespace gd {
+
+gd_status fail(gd_status st, const char *fmt, ...);
+
+#define GD_CUDA(call)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return ::gd::fail(e_ == cudaErrorMemoryAllocation ? GD_ENOMEM : GD_ECUDA,          \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,      \
+                        __LINE__);                                                      \
+  } while (0)
+
+#define GD_TRY(call)            \
+  do {                          \
+    gd_status s_ = (call);      \
+    if (s_ != GD_OK) return s_; \
+  } while (0)
+
+constexpr float kPI = 3.1415926535f;  // size.h:86
+
+// Launch shape of the energy kernel: A atom groups x P tile groups of warps,
+// NA ligand atoms per warp.
+struct Tile {
+  int A = 0, P = 0, NA = 0;
+  bool valid() const { return A > 0 && P > 0 && NA > 0; }
+};
+
+// Candidate atoms-per-warp values compiled into the kernel.
+constexpr int kNAValues[] = {1, 2, 3, 4, 5, 6, 8, 10};
+
+Tile default_tile(int lna, bool resident);
+int round_na(int na);  // smallest compiled NA >= na (0 if none)
+void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident);
+
+}  // namespace gd
+
+// Handles are reference counted: a complex keeps its context (and a shared
+// protein's owner) alive, a REMC run or batch keeps its complexes alive, so
+// callers may destroy them in any order.
+struct gd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int *d_err = nullptr;
+  uint64_t launches = 0;
+  int n_sm = 148;
+  std::atomic<int> refs{1};
+  // autotuned launch shapes keyed by (ligand atoms, protein tiles)
+  std::mutex tile_mu;
+  std::map<std::pair<int, int>, gd::Tile> tiles;
+};
+
+struct gd_dcomplex {
+  gd_ctx *ctx = nullptr;
+  gd::KTables T{};
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+  std::atomic<int> refs{1};
+  gd_dcomplex *protein_owner = nullptr;  // when the protein arrays are shared
+};
+
+namespace gd {
+void ctx_retain(gd_ctx *c);
+void ctx_release(gd_ctx *c);
+void dcx_retain(gd_dcomplex *d);
+void dcx_release(gd_dcomplex *d);
+gd_status ctx_check(gd_ctx *c);
+Tile tile_for(gd_ctx *ctx, const KTables &T);
+}  // namespace gd

@@ -1,0 +1,603 @@
+// gd_ensemble.cu -- replica-exchange Monte Carlo runs: the plain per-complex
+// form (gd_remc, one complex) and the batched form (gd_batch, many complexes
+// of uneven sizes advanced together), both built on one launch planner.
+//
+// Reference path replaced: the Run() loop of gpudocksm-rem-1.2/src/run.cu and
+// gpusingle.cu:5-37 (MonteCarlo_d launches of steps_per_exchange steps, each
+// followed by a single-thread ExchangeReplicas_d, all synchronous).
+//
+// Planning: every complex gets a launch shape (A x P warps, NA atoms per
+// warp; from the context's autotuned table or the default), complexes with
+// the same shape share one launch.  When the temperature count divides 32 a
+// CTA holds whole exchange groups (32 / n_tmp ligand conformations x all
+// temperatures) and the exchange runs inside the kernel, so a run of any
+// length is one launch per shape; otherwise an exchange kernel follows every
+// interval.  The per-interval launch sequence reads its first MC step from a
+// device counter, so it is captured once into a CUDA graph and replayed.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gd_common.h"
+
+using namespace gd;
+
+namespace {
+
+struct Plan {
+  Tile tile;
+  int n_stages = 0, resident = 0, group_major = 0, fused = 0, grid = 0;
+  int *d_cta_item = nullptr, *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
+};
+
+struct Ens {
+  gd_ctx *ctx = nullptr;
+  std::vector<gd_dcomplex *> dcx;
+  std::vector<gd_mc_params> mc;
+  std::vector<KItem> items;
+  KItem *d_items = nullptr;
+  int n_rep_total = 0, spe = 0, step = 0;
+  float *m_old = nullptr, *e_old = nullptr, *minus_beta = nullptr;
+  int *idx_tmp = nullptr, *acs_mc = nullptr, *acs_exchg = nullptr, *d_step = nullptr;
+  std::vector<Plan> plans;
+  KGroup *d_groups = nullptr;
+  int n_groups = 0;  // groups exchanged by the separate kernel
+  bool all_fused = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool profile = false;
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_kind;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timing = false;
+  double t_compute = 0.0;
+  std::vector<void *> allocs;
+};
+
+template <typename T>
+gd_status dalloc(Ens &E, T **out, size_t n) {
+  void *p = nullptr;
+  GD_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  E.allocs.push_back(p);
+  GD_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), E.ctx->stream));
+  *out = (T *)p;
+  return GD_OK;
+}
+
+template <typename T>
+gd_status dcopy(Ens &E, T **out, const std::vector<T> &h) {
+  GD_TRY(dalloc(E, out, h.size()));
+  if (!h.empty())
+    GD_CUDA(cudaMemcpyAsync(*out, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice,
+                            E.ctx->stream));
+  return GD_OK;
+}
+
+gd_status validate_mc(const gd_mc_params *mc) {
+  if (!mc) return fail(GD_EINVAL, "mc params NULL");
+  if (mc->n_tmp < 1 || mc->n_tmp > MAX_TMP)
+    return fail(GD_EINVAL, "n_tmp=%d outside [1, %d]", mc->n_tmp, MAX_TMP);
+  if (!mc->minus_beta) return fail(GD_EINVAL, "minus_beta NULL");
+  if (mc->steps_total < 0) return fail(GD_EINVAL, "steps_total=%d", mc->steps_total);
+  if (mc->steps_per_exchange < 1)
+    return fail(GD_EINVAL, "steps_per_exchange=%d", mc->steps_per_exchange);
+  if (mc->steps_total % mc->steps_per_exchange != 0)
+    return fail(GD_EINVAL, "steps_total %d is not a multiple of steps_per_exchange %d",
+                mc->steps_total, mc->steps_per_exchange);
+  for (int i = 0; i < mc->n_tmp; ++i)
+    if (!std::isfinite(mc->minus_beta[i])) return fail(GD_EINVAL, "minus_beta[%d] not finite", i);
+  return GD_OK;
+}
+
+void ens_free(Ens &E) {
+  if (E.ctx) {
+    cudaSetDevice(E.ctx->device);
+    cudaStreamSynchronize(E.ctx->stream);
+  }
+  if (E.gexec) cudaGraphExecDestroy(E.gexec);
+  if (E.graph) cudaGraphDestroy(E.graph);
+  for (void *p : E.allocs) cudaFree(p);
+  for (cudaEvent_t e : E.prof_ev) cudaEventDestroy(e);
+  if (E.ev0) cudaEventDestroy(E.ev0);
+  if (E.ev1) cudaEventDestroy(E.ev1);
+  for (gd_dcomplex *d : E.dcx) dcx_release(d);
+  E.dcx.clear();
+  ctx_release(E.ctx);
+  E.ctx = nullptr;
+}
+
+gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
+                    const gd_mc_params *mc) {
+  E.ctx = ctx;
+  ctx_retain(ctx);
+  if (n < 1) return fail(GD_EINVAL, "no complexes");
+  E.spe = mc[0].steps_per_exchange;
+  for (int i = 0; i < n; ++i) {
+    if (!dcx[i]) return fail(GD_EINVAL, "complex %d is NULL", i);
+    if (dcx[i]->ctx != ctx) return fail(GD_EINVAL, "complex %d belongs to another context", i);
+    GD_TRY(validate_mc(&mc[i]));
+    if (mc[i].steps_per_exchange != E.spe)
+      return fail(GD_EINVAL, "complex %d: steps_per_exchange %d differs from %d", i,
+                  mc[i].steps_per_exchange, E.spe);
+    E.dcx.push_back(const_cast<gd_dcomplex *>(dcx[i]));
+    dcx_retain(E.dcx.back());
+    E.mc.push_back(mc[i]);
+  }
+  // replica layout and per-item state
+  E.items.resize(n);
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    const KTables &T = E.dcx[i]->T;
+    KItem &I = E.items[i];
+    I.T = T;
+    I.n_tmp = mc[i].n_tmp;
+    I.n_lig_conf = T.n_lig;
+    I.n_prt = T.n_prt;
+    I.n_rep = T.n_prt * T.n_lig * mc[i].n_tmp;
+    I.rep_base = (int)total;
+    I.steps_per_dump = mc[i].steps_per_dump;
+    I.rec_steps = 0;
+    for (int k = 0; k < 6; ++k) I.move_scale[k] = mc[i].move_scale[k];
+    I.seed = mc[i].seed;
+    I.stream_id = mc[i].stream_id;
+    I.flags = mc[i].flags;
+    total += I.n_rep;
+  }
+  if (total > (1LL << 30)) return fail(GD_EINVAL, "too many replicas: %lld", total);
+  E.n_rep_total = (int)total;
+  GD_TRY(dalloc(E, &E.m_old, (size_t)total * 6));
+  GD_TRY(dalloc(E, &E.e_old, (size_t)total * GD_NTERM));
+  GD_TRY(dalloc(E, &E.idx_tmp, (size_t)total));
+  GD_TRY(dalloc(E, &E.acs_mc, (size_t)total));
+  GD_TRY(dalloc(E, &E.acs_exchg, (size_t)n * MAX_TMP));
+  GD_TRY(dalloc(E, &E.d_step, 1));
+  {
+    std::vector<float> mb((size_t)n * MAX_TMP, 0.f);
+    for (int i = 0; i < n; ++i)
+      std::copy(mc[i].minus_beta, mc[i].minus_beta + mc[i].n_tmp, mb.begin() + (size_t)i * MAX_TMP);
+    GD_TRY(dcopy(E, &E.minus_beta, mb));
+  }
+  for (int i = 0; i < n; ++i) {
+    KItem &I = E.items[i];
+    I.minus_beta = E.minus_beta + (size_t)i * MAX_TMP;
+    I.acs_exchg = E.acs_exchg + (size_t)i * MAX_TMP;
+    I.record = nullptr;
+    if (mc[i].flags & GD_MC_RECORD) {
+      gd_record *rec = nullptr;
+      GD_TRY(dalloc(E, &rec, (size_t)I.n_rep * std::max(1, mc[i].steps_total)));
+      I.record = rec;
+      I.rec_steps = mc[i].steps_total;
+    }
+  }
+  GD_TRY(dcopy(E, &E.d_items, E.items));
+
+  // launch plans: one per (shape, staging, layout); CTAs in decreasing cost
+  using Key = std::tuple<int, int, int, int, int, int>;
+  std::map<Key, std::vector<std::tuple<double, int, int, int>>> ctas;  // cost, item, rep0, n
+  std::map<Key, Plan> plans;
+  std::vector<KGroup> groups;
+  for (int i = 0; i < n; ++i) {
+    const KItem &I = E.items[i];
+    Tile t = tile_for(ctx, I.T);
+    int ns, res;
+    pick_stages(I.T, t, &ns, &res);
+    if (!res) t.P = 1;
+    const int nt = I.n_tmp, nl = I.n_lig_conf;
+    const bool gm = (32 % nt) == 0;
+    const bool exch = (I.flags & GD_MC_EXCHANGE) != 0;
+    const Key key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0};
+    Plan &pl = plans[key];
+    pl.tile = t;
+    pl.n_stages = ns;
+    pl.resident = res;
+    pl.group_major = gm ? 1 : 0;
+    pl.fused = gm ? 1 : 0;
+    const double cost = (double)I.T.lna * I.T.pnp;
+    auto &list = ctas[key];
+    if (gm) {
+      const int G = 32 / nt;
+      for (int p = 0; p < I.n_prt; ++p)
+        for (int l0 = 0; l0 < nl; l0 += G)
+          list.emplace_back(cost, i, p * nl + l0, std::min(G, nl - l0) * nt);
+    } else {
+      const int per_p = nt * nl;
+      for (int p = 0; p < I.n_prt; ++p)
+        for (int j = 0; j < per_p; j += 32)
+          list.emplace_back(cost, i, p * per_p + j, std::min(32, per_p - j));
+      if (exch) {
+        E.all_fused = false;
+        for (int p = 0; p < I.n_prt; ++p)
+          for (int l = 0; l < nl; ++l) groups.push_back(KGroup{i, p, l, 0});
+      }
+    }
+  }
+  for (auto &kv : plans) {
+    Plan pl = kv.second;
+    auto &list = ctas[kv.first];
+    std::stable_sort(list.begin(), list.end(),
+                     [](const auto &a, const auto &b) { return std::get<0>(a) > std::get<0>(b); });
+    std::vector<int> ci, c0, cn;
+    for (auto &c : list) {
+      ci.push_back(std::get<1>(c));
+      c0.push_back(std::get<2>(c));
+      cn.push_back(std::get<3>(c));
+    }
+    pl.grid = (int)ci.size();
+    GD_TRY(dcopy(E, &pl.d_cta_item, ci));
+    GD_TRY(dcopy(E, &pl.d_cta_rep0, c0));
+    GD_TRY(dcopy(E, &pl.d_cta_nrep, cn));
+    E.plans.push_back(pl);
+  }
+  E.n_groups = (int)groups.size();
+  if (E.n_groups) GD_TRY(dcopy(E, &E.d_groups, groups));
+  GD_CUDA(cudaEventCreate(&E.ev0));
+  GD_CUDA(cudaEventCreate(&E.ev1));
+  GD_CUDA(cudaStreamSynchronize(ctx->stream));
+  return GD_OK;
+}
+
+KRun run_desc(const Ens &E, const Plan &pl, int mode) {
+  KRun R{};
+  R.mode = mode;
+  R.A = pl.tile.A;
+  R.P = pl.tile.P;
+  R.n_stages = pl.n_stages;
+  R.resident = pl.resident;
+  R.items = E.d_items;
+  R.cta_item = pl.d_cta_item;
+  R.cta_rep0 = pl.d_cta_rep0;
+  R.cta_nrep = pl.d_cta_nrep;
+  R.group_major = pl.group_major;
+  R.fused_exchange = pl.fused;
+  R.spe = E.spe;
+  R.m_old = E.m_old;
+  R.e_old = E.e_old;
+  R.idx_tmp = E.idx_tmp;
+  R.acs_mc = E.acs_mc;
+  R.err = E.ctx->d_err;
+  return R;
+}
+
+gd_status mark(Ens &E, int kind) {
+  cudaEvent_t e;
+  GD_CUDA(cudaEventCreate(&e));
+  E.prof_ev.push_back(e);
+  E.prof_kind.push_back(kind);
+  GD_CUDA(cudaEventRecord(e, E.ctx->stream));
+  return GD_OK;
+}
+
+gd_status ens_init(Ens &E) {
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  cudaStream_t s = E.ctx->stream;
+  GD_CUDA(cudaMemsetAsync(E.acs_exchg, 0, sizeof(int) * MAX_TMP * E.items.size(), s));
+  GD_CUDA(cudaMemsetAsync(E.d_step, 0, sizeof(int), s));
+  for (const Plan &pl : E.plans) {
+    KRun R = run_desc(E, pl, KMODE_INIT);
+    R.step0 = 0;
+    R.n_steps = 1;
+    GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
+    E.ctx->launches += 1;
+  }
+  E.step = 0;
+  E.t_compute = 0.0;
+  return GD_OK;
+}
+
+// The launches of `k` intervals.  With a device step counter (graph mode)
+// every launch reads its first step from it and the last node advances it.
+gd_status ens_enqueue(Ens &E, int n_steps, bool device_step) {
+  cudaStream_t s = E.ctx->stream;
+  if (E.all_fused) {
+    // exchanges happen inside the kernel: one launch per plan for the run
+    for (const Plan &pl : E.plans) {
+      KRun R = run_desc(E, pl, KMODE_REMC);
+      R.step0 = E.step;
+      R.n_steps = n_steps;
+      R.step_ptr = device_step ? E.d_step : nullptr;
+      if (E.profile) GD_TRY(mark(E, 0));
+      GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
+      if (E.profile) GD_TRY(mark(E, 0));
+      E.ctx->launches += 1;
+    }
+    if (device_step) {
+      GD_CUDA(launch_advance(E.d_step, n_steps, s));
+      E.ctx->launches += 1;
+    }
+    return GD_OK;
+  }
+  for (int s0 = E.step; s0 < E.step + n_steps; s0 += E.spe) {
+    for (const Plan &pl : E.plans) {
+      KRun R = run_desc(E, pl, KMODE_REMC);
+      R.step0 = s0;
+      R.n_steps = E.spe;
+      R.step_ptr = device_step ? E.d_step : nullptr;
+      if (E.profile) GD_TRY(mark(E, 0));
+      GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
+      if (E.profile) GD_TRY(mark(E, 0));
+      E.ctx->launches += 1;
+    }
+    if (E.n_groups) {
+      if (E.profile) GD_TRY(mark(E, 1));
+      GD_CUDA(launch_exchange(E.d_items, E.d_groups, E.n_groups, E.e_old, E.idx_tmp, E.spe, s0,
+                              device_step ? E.d_step : nullptr, s));
+      if (E.profile) GD_TRY(mark(E, 1));
+      E.ctx->launches += 1;
+    }
+    if (device_step) {
+      GD_CUDA(launch_advance(E.d_step, E.spe, s));
+      E.ctx->launches += 1;
+    }
+  }
+  return GD_OK;
+}
+
+gd_status ens_run(Ens &E, int n_steps) {
+  if (n_steps < 0 || n_steps % E.spe != 0)
+    return fail(GD_EINVAL, "n_steps %d is not a multiple of steps_per_exchange %d", n_steps,
+                E.spe);
+  if (n_steps == 0) return GD_OK;
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  cudaStream_t s = E.ctx->stream;
+  GD_CUDA(cudaEventRecord(E.ev0, s));
+  // keep the device step counter in step with the host's
+  GD_CUDA(cudaMemcpyAsync(E.d_step, &E.step, sizeof(int), cudaMemcpyHostToDevice, s));
+  if (E.all_fused || E.profile) {
+    GD_TRY(ens_enqueue(E, n_steps, false));
+  } else {
+    // one captured interval, replayed n_steps / spe times
+    if (!E.gexec) {
+      GD_CUDA(cudaStreamSynchronize(s));
+      GD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int saved = E.step;
+      const uint64_t l0 = E.ctx->launches;
+      gd_status st = ens_enqueue(E, E.spe, true);
+      E.step = saved;
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (st != GD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+      }
+      if (ce != cudaSuccess) return fail(GD_ECUDA, "graph capture: %s", cudaGetErrorString(ce));
+      E.graph = g;
+      GD_CUDA(cudaGraphInstantiate(&E.gexec, g, 0));
+      E.ctx->launches = l0;  // counted when replayed
+    }
+    const int per_graph = (int)E.plans.size() + (E.n_groups ? 1 : 0) + 1;
+    for (int k = 0; k < n_steps / E.spe; ++k) {
+      GD_CUDA(cudaGraphLaunch(E.gexec, s));
+      E.ctx->launches += per_graph;
+    }
+  }
+  GD_CUDA(cudaEventRecord(E.ev1, s));
+  E.timing = true;
+  E.step += n_steps;
+  return GD_OK;
+}
+
+gd_status ens_read(Ens &E, int i, gd_mc_log *log) {
+  if (i < 0 || i >= (int)E.items.size()) return fail(GD_EINVAL, "item %d out of range", i);
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  GD_TRY(ctx_check(E.ctx));
+  if (E.timing) {
+    float ms = 0.f;
+    GD_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
+    E.t_compute += ms * 1e-3;
+    E.timing = false;
+  }
+  const KItem &I = E.items[i];
+  const size_t n = (size_t)I.n_rep, b = (size_t)I.rep_base;
+  std::vector<int> acs(n), acx(I.n_tmp);
+  cudaStream_t s = E.ctx->stream;
+  GD_CUDA(cudaMemcpyAsync(acs.data(), E.acs_mc + b, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(acx.data(), I.acs_exchg, sizeof(int) * I.n_tmp, cudaMemcpyDeviceToHost,
+                          s));
+  if (log->energy)
+    GD_CUDA(cudaMemcpyAsync(log->energy, E.e_old + b * GD_NTERM, sizeof(float) * GD_NTERM * n,
+                            cudaMemcpyDeviceToHost, s));
+  if (log->movematrix)
+    GD_CUDA(cudaMemcpyAsync(log->movematrix, E.m_old + b * 6, sizeof(float) * 6 * n,
+                            cudaMemcpyDeviceToHost, s));
+  if (log->idx_tmp)
+    GD_CUDA(cudaMemcpyAsync(log->idx_tmp, E.idx_tmp + b, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                            s));
+  if (log->record && I.record)
+    GD_CUDA(cudaMemcpyAsync(log->record, I.record, sizeof(gd_record) * n * std::max(1, I.rec_steps),
+                            cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaStreamSynchronize(s));
+  log->ac_mc = 0;
+  for (size_t k = 0; k < n; ++k) log->ac_mc += acs[k];
+  log->ac_temp_exchg = 0;
+  for (int t = 0; t < I.n_tmp; ++t) log->ac_temp_exchg += acx[t];
+  if (log->acs_mc) std::memcpy(log->acs_mc, acs.data(), sizeof(int) * n);
+  if (log->acs_temp_exchg) std::memcpy(log->acs_temp_exchg, acx.data(), sizeof(int) * I.n_tmp);
+  log->t_compute = E.t_compute;
+  return GD_OK;
+}
+
+gd_status ens_kernel_times(Ens &E, double *mc_ms, int *mc_n, double *ex_ms, int *ex_n) {
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  GD_CUDA(cudaStreamSynchronize(E.ctx->stream));
+  *mc_ms = *ex_ms = 0.0;
+  *mc_n = *ex_n = 0;
+  for (size_t i = 0; i + 1 < E.prof_ev.size(); i += 2) {
+    float ms = 0.f;
+    GD_CUDA(cudaEventElapsedTime(&ms, E.prof_ev[i], E.prof_ev[i + 1]));
+    if (E.prof_kind[i] == 0) {
+      *mc_ms += ms;
+      *mc_n += 1;
+    } else {
+      *ex_ms += ms;
+      *ex_n += 1;
+    }
+  }
+  for (cudaEvent_t e : E.prof_ev) cudaEventDestroy(e);
+  E.prof_ev.clear();
+  E.prof_kind.clear();
+  return GD_OK;
+}
+
+}  // namespace
+
+struct gd_remc {
+  Ens e;
+};
+struct gd_batch {
+  Ens e;
+};
+
+// ---------------------------------------------------------------------------
+// Plain form: one complex
+// ---------------------------------------------------------------------------
+extern "C" gd_status gd_remc_create(gd_ctx *ctx, const gd_dcomplex *d, const gd_mc_params *mc,
+                                    gd_remc **out) {
+  if (!ctx || !d || !out) return fail(GD_EINVAL, "gd_remc_create: NULL argument");
+  *out = nullptr;
+  GD_TRY(validate_mc(mc));
+  GD_CUDA(cudaSetDevice(ctx->device));
+  gd_remc *r = new (std::nothrow) gd_remc;
+  if (!r) return fail(GD_ENOMEM, "host allocation");
+  gd_status st;
+  try {
+    st = ens_build(r->e, ctx, 1, &d, mc);
+  } catch (const std::bad_alloc &) {
+    st = fail(GD_ENOMEM, "host allocation");
+  }
+  if (st != GD_OK) {
+    ens_free(r->e);
+    delete r;
+    return st;
+  }
+  *out = r;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_remc_destroy(gd_remc *r) {
+  if (!r) return GD_OK;
+  ens_free(r->e);
+  delete r;
+  return GD_OK;
+}
+
+extern "C" int gd_remc_n_rep(const gd_remc *r) { return r ? r->e.n_rep_total : 0; }
+
+extern "C" gd_status gd_remc_init(gd_remc *r) {
+  if (!r) return fail(GD_EINVAL, "remc NULL");
+  return ens_init(r->e);
+}
+
+extern "C" gd_status gd_remc_run(gd_remc *r, int n_steps) {
+  if (!r) return fail(GD_EINVAL, "remc NULL");
+  return ens_run(r->e, n_steps);
+}
+
+extern "C" gd_status gd_remc_read(gd_remc *r, gd_mc_log *log) {
+  if (!r || !log) return fail(GD_EINVAL, "gd_remc_read: NULL argument");
+  return ens_read(r->e, 0, log);
+}
+
+extern "C" gd_status gd_remc_set_profiling(gd_remc *r, int on) {
+  if (!r) return fail(GD_EINVAL, "remc NULL");
+  r->e.profile = on != 0;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_remc_kernel_times(gd_remc *r, double *mc_ms, int *mc_launches,
+                                          double *exch_ms, int *exch_launches) {
+  if (!r || !mc_ms || !mc_launches || !exch_ms || !exch_launches)
+    return fail(GD_EINVAL, "gd_remc_kernel_times: NULL argument");
+  return ens_kernel_times(r->e, mc_ms, mc_launches, exch_ms, exch_launches);
+}
+
+extern "C" gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log) {
+  const auto t0 = std::chrono::steady_clock::now();
+  GD_TRY(validate_mc(mc));
+  gd_ctx *ctx = nullptr;
+  GD_TRY(gd_ctx_create(0, nullptr, &ctx));
+  gd_dcomplex *d = nullptr;
+  gd_remc *r = nullptr;
+  gd_status st = gd_complex_upload(ctx, cx, &d);
+  if (st == GD_OK) st = gd_remc_create(ctx, d, mc, &r);
+  if (st == GD_OK) st = gd_remc_init(r);
+  if (st == GD_OK) st = gd_remc_run(r, mc->steps_total);
+  if (st == GD_OK && log) st = gd_remc_read(r, log);
+  gd_remc_destroy(r);
+  gd_complex_free(d);
+  gd_ctx_destroy(ctx);
+  if (st == GD_OK && log)
+    log->t_wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: many complexes (uneven sizes) advanced together
+// ---------------------------------------------------------------------------
+extern "C" gd_status gd_batch_create(gd_ctx *ctx, int n, const gd_dcomplex *const *items,
+                                     const gd_mc_params *params, gd_batch **out) {
+  if (!ctx || !items || !params || !out) return fail(GD_EINVAL, "gd_batch_create: NULL argument");
+  *out = nullptr;
+  GD_CUDA(cudaSetDevice(ctx->device));
+  gd_batch *b = new (std::nothrow) gd_batch;
+  if (!b) return fail(GD_ENOMEM, "host allocation");
+  gd_status st;
+  try {
+    st = ens_build(b->e, ctx, n, items, params);
+  } catch (const std::bad_alloc &) {
+    st = fail(GD_ENOMEM, "host allocation");
+  }
+  if (st != GD_OK) {
+    ens_free(b->e);
+    delete b;
+    return st;
+  }
+  *out = b;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_batch_destroy(gd_batch *b) {
+  if (!b) return GD_OK;
+  ens_free(b->e);
+  delete b;
+  return GD_OK;
+}
+
+extern "C" int gd_batch_n_rep(const gd_batch *b) { return b ? b->e.n_rep_total : 0; }
+extern "C" int gd_batch_n_launch_shapes(const gd_batch *b) {
+  return b ? (int)b->e.plans.size() : 0;
+}
+
+extern "C" gd_status gd_batch_init(gd_batch *b) {
+  if (!b) return fail(GD_EINVAL, "batch NULL");
+  return ens_init(b->e);
+}
+
+extern "C" gd_status gd_batch_run(gd_batch *b, int n_steps) {
+  if (!b) return fail(GD_EINVAL, "batch NULL");
+  return ens_run(b->e, n_steps);
+}
+
+extern "C" gd_status gd_batch_read(gd_batch *b, int item, gd_mc_log *log) {
+  if (!b || !log) return fail(GD_EINVAL, "gd_batch_read: NULL argument");
+  return ens_read(b->e, item, log);
+}
+
+extern "C" gd_status gd_batch_set_profiling(gd_batch *b, int on) {
+  if (!b) return fail(GD_EINVAL, "batch NULL");
+  b->e.profile = on != 0;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_batch_kernel_times(gd_batch *b, double *mc_ms, int *mc_launches,
+                                           double *exch_ms, int *exch_launches) {
+  if (!b || !mc_ms || !mc_launches || !exch_ms || !exch_launches)
+    return fail(GD_EINVAL, "gd_batch_kernel_times: NULL argument");
+  return ens_kernel_times(b->e, mc_ms, mc_launches, exch_ms, exch_launches);
+}

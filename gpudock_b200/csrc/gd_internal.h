@@ -1,5 +1,5 @@
 // gd_internal.h -- device data layout and kernel launch descriptors shared by
-// the host API (gd_api.cu) and the kernels (gd_kernels.cu).
+// the host API (gd_api.cu, gd_batch.cu) and the kernels (gd_kernels.cu).
 #pragma once
 
 #include <cstdint>
@@ -9,15 +9,17 @@
 
 namespace gd {
 
-// Protein points are streamed through shared memory in tiles of TILE_PTS
+// Protein points are staged through shared memory in tiles of TILE_PTS
 // points: a 16-byte record {x, y, z, ele} and an 8-byte record {hpp, meta}.
 constexpr int TILE_PTS = 128;
 constexpr int STREAM_STAGES = 8;       // ring depth when the protein streams
-constexpr int MAX_RESIDENT_TILES = 56; // 7168 points kept in smem for the run
-constexpr int MAX_WARPS = 16;          // compute warps per CTA
-constexpr int MAX_APW = 8;             // ligand atoms per warp per pass
+constexpr int MAX_RESIDENT_TILES = 56; // 7168 points kept in smem for a launch
+constexpr int MAX_WARPS = 12;          // compute warps per CTA (plus 1 producer)
+constexpr int MAX_NA = 10;             // ligand atoms per warp (template bound)
+constexpr int MAX_LNA = 128;           // ligand atoms per complex
 constexpr int NRED = 8;                // partial sums per replica per warp
 constexpr int MAX_TMP = 64;            // temperatures per exchange group
+constexpr int TAB_ROWS = GD_NLT + 1;   // + one all-zero row for padding atoms
 
 // meta word of a protein point: type | class << 5 | hpc flag << 8 |
 // seq3r << 12 (seq3r < 2^20)
@@ -29,12 +31,12 @@ constexpr int MAX_SEQ3R = (1 << 20) - 1;
 
 enum KMode : int { KMODE_POSES = 0, KMODE_REMC = 1, KMODE_INIT = 2 };
 
-// Everything the energy needs, device pointers + scalars (by value).
+// Tables of one complex (device pointers + scalars).
 struct KTables {
   const float4 *pt_a;   // [n_prt][pnp_pad] {x, y, z, ele}
   const float2 *pt_b;   // [pnp_pad] {hpp, meta bits}
-  const float4 *tab_a;  // [NLT*NPT] {p1a, p2a, pmf0, pmf1}
-  const float2 *tab_b;  // [NLT*NPT] {hdb0, hdb1}
+  const float4 *tab_a;  // [TAB_ROWS*NPT] {p1a, p2a, pmf0, pmf1}
+  const float2 *tab_b;  // [TAB_ROWS*NPT] {hdb0, hdb1}
   const float4 *lig;    // [n_lig][lna] {x, y, z, 0} relative to the centre
   const int *lig_t;     // [lna]
   const float *lig_q;   // [lna]
@@ -46,53 +48,74 @@ struct KTables {
   const float *mcs_cnt; // [pos] number of valid atoms (float)
   int lna, n_lig, pnp, pnp_pad, n_prt, pos, psp_ncol, pad0;
   float lj0, lj0lj1, el0, el1, inv_el1, a1, b1, kde2, kde3;
-  float s2pi;           // sqrtf(2 * 3.1415926535f), as the reference's float
+  float s2pi;           // sqrtf(2 * 3.1415926535f), the reference's float
+  float near_d2;        // squared distance below which a rare term can fire
   float hpl0[GD_NLT], hpl1[GD_NLT], hpl2[GD_NLT];
   float a_para[GD_NTERM], b_para[GD_NTERM], w[GD_NTERM];
   float lig_center[3], pocket[3];
 };
 
-// Replica state of a REMC run on the device.
-struct KState {
-  float *m_old;         // [n_rep][6]
-  float *e_old;         // [n_rep][GD_NTERM]
-  int *idx_tmp;         // [n_rep]
-  int *acs_mc;          // [n_rep]
-  int *acs_exchg;       // [n_tmp] by slot
-  gd_record *record;    // [n_rep][rec_steps] or nullptr
-  const float *minus_beta;  // [n_tmp]
-  int n_rep, n_tmp, n_lig_conf, rec_steps;
-};
-
-// Launch descriptor of one dock_kernel launch.
-struct KRun {
-  int mode;             // KMode
-  int n_warps;          // compute warps
-  int n_stages;         // smem tile stages (== n_tiles when resident)
-  int resident;         // 1: whole protein conformation kept in smem
-  // poses
-  int prt_conf, lig_conf, n_pose;
-  const float *poses;   // [n_pose][6]
-  float *terms;         // [n_pose][GD_NTERM]
-  double *raw;          // [n_pose][GD_NRAW] or nullptr
-  // REMC
-  const int *cta_rep0;  // [grid] first replica of each CTA
-  const int *cta_nrep;  // [grid] replicas of each CTA (<= 32, same protein conf)
-  int step0, n_steps;
+// One complex of a launch with its Monte Carlo parameters and the location
+// of its replicas in the launch-wide state arrays.
+struct KItem {
+  KTables T;
+  int rep_base;          // first replica of this item in the state arrays
+  int n_rep, n_tmp, n_lig_conf, n_prt;
+  int steps_per_dump;    // exchange parity restarts every dump (<= 0: never)
+  int rec_steps;
+  int pad1;
   float move_scale[6];
   uint64_t seed;
-  uint32_t stream_id;
-  uint32_t flags;
-  KState st;
-  int *err;             // error word (bounded waits)
+  uint32_t stream_id, flags;
+  const float *minus_beta;  // [n_tmp]
+  int *acs_exchg;           // [n_tmp] by slot
+  gd_record *record;        // [n_rep][rec_steps] or nullptr
 };
 
-size_t dock_smem_bytes(int n_warps, int n_stages);
+// Launch descriptor of one dock_kernel launch (by value).
+struct KRun {
+  int mode;              // KMode
+  int A, P;              // warp grid: A atom groups x P protein-tile groups
+  int n_stages;          // smem tile stages (== n_tiles when resident)
+  int resident;          // 1: whole protein conformation kept in smem
+  const KItem *items;
+  const int *cta_item;   // [grid] item of each CTA (REMC / INIT)
+  const int *cta_rep0;   // [grid] first local replica of each CTA, or with
+                         // group_major the first exchange group p*n_lig + l
+  const int *cta_nrep;   // [grid] replicas of each CTA (<= 32, one protein conf)
+  int group_major;       // lane = (group g0 + lane / n_tmp, temperature slot
+                         // lane % n_tmp): whole exchange groups per CTA
+  int fused_exchange;    // group_major only: exchange inside the kernel after
+                         // every spe MC steps
+  int spe;               // MC steps per exchange
+  // poses (item 0)
+  int prt_conf, lig_conf, n_pose;
+  const float *poses;    // [n_pose][6]
+  float *terms;          // [n_pose][GD_NTERM]
+  double *raw;           // [n_pose][GD_NRAW] or nullptr
+  // REMC: the first MC step is *step_ptr when step_ptr is set (graph replay)
+  int step0, n_steps;
+  const int *step_ptr;
+  float *m_old;          // [n_rep_total][6]
+  float *e_old;          // [n_rep_total][GD_NTERM]
+  int *idx_tmp;          // [n_rep_total]
+  int *acs_mc;           // [n_rep_total]
+  int *err;              // error word (bounded waits)
+};
+
+// Exchange groups: one (item, protein conf, ligand conf) each.
+struct KGroup {
+  int item, p, l, pad;
+};
+
+size_t dock_smem_bytes(int A, int P, int NA, int n_stages);
 
 // Kernel launchers (gd_kernels.cu); return the launch status.
-cudaError_t launch_dock(const KTables &T, const KRun &R, int grid, cudaStream_t s);
-cudaError_t launch_exchange(const KState &S, int n_prt, int n_lig, uint64_t seed,
-                            uint32_t stream_id, int round, int mode_t, cudaStream_t s);
+cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s);
+cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups,
+                            const float *e_old, int *idx_tmp, int spe, int step0,
+                            const int *step_ptr, cudaStream_t s);
+cudaError_t launch_advance(int *step_ptr, int spe, cudaStream_t s);
 cudaError_t launch_metropolis(int n, const float *e_new, const float *e_old,
                               const float *mbeta, const int *rep, const int *step,
                               uint64_t seed, uint32_t stream_id, int *acc, cudaStream_t s);

@@ -1,15 +1,24 @@
 // gd_kernels.cu -- sm_100a kernels of the REMC docking path.
 //
-// dock_kernel: one CTA owns up to 32 replicas (or poses) that share one
-// protein conformation; lane i of every compute warp is replica i, so all
-// protein-point and type-table reads are warp-uniform shared-memory
-// broadcasts.  The ligand atoms are split across the compute warps (atom
-// a = warp + W*k, kept in registers), the protein conformation is staged in
-// shared memory in 128-point tiles by the TMA engine (cp.async.bulk +
-// mbarrier), either once for the whole launch (resident) or through an
-// 8-stage ring fed by a producer warp.  Per step each warp writes FP64 partial
-// sums per replica; warp 0 reduces them, normalises the terms, and takes the
-// Metropolis decision with the counter-based RNG.
+// dock_kernel: one CTA owns up to 32 replicas (or poses) of one complex that
+// share one protein conformation; lane i of every compute warp is replica i,
+// so protein-point and type-table reads are warp-uniform shared-memory
+// broadcasts.  The compute warps form an A x P grid: warp (ag, pg) keeps NA
+// ligand atoms a = ag + A k in registers and sweeps the protein tiles
+// t = pg, pg + P, ...  The protein conformation is staged in shared memory in
+// 128-point tiles by the TMA engine (cp.async.bulk + mbarrier), once per
+// launch when it fits (resident) or through an 8-stage ring fed by a
+// producer warp (then P = 1).  Per step every warp writes FP64 partial sums
+// per replica; warp 0 reduces them in a fixed order, normalises the terms
+// and takes the Metropolis decision with the counter-based RNG.
+//
+// Per ligand-protein pair the fast path evaluates the terms every pair
+// contributes to (soft LJ, far-field electrostatics, contact PMF) with one
+// rsqrt, two reciprocals and one exp2.  The terms that only fire close in
+// (hydrophobic contact d <= 9 A, near-field electrostatics d < 1/el1,
+// pocket-specific potential d <= pmf0) run only when some lane has an atom
+// within near_d2 of the point; the H-bond term runs for the type pairs that
+// define one.
 //
 // Reference semantics (gpudocksm-rem-1.2/src):
 //   pair terms          calcenergy_d.cu:56-138
@@ -29,15 +38,51 @@
 
 namespace gd {
 
-constexpr int TAB_N = GD_NLT * GD_NPT;
+constexpr int TAB_N = TAB_ROWS * GD_NPT;
 constexpr int TAB_BYTES = TAB_N * (16 + 8);
 constexpr int STAGE_BYTES = TILE_PTS * (16 + 8);
 constexpr int CHUNK = 32;  // points per FP32 partial before the FP64 flush
+constexpr float LOG2E = 1.4426950408889634f;
+constexpr float FAR = 1.0e4f;  // coordinate of the padding atoms
 
-size_t dock_smem_bytes(int n_warps, int n_stages) {
+// Per-replica state in shared memory, written by warp 0 only.
+struct LaneState {
+  float m_old[6];
+  float m_new[6];
+  float rot[9];
+  float e_old[GD_NTERM];
+  float mbeta;       // -1/T of the replica's current temperature
+  int idx_tmp;       // its temperature index
+  int acs;           // accepted moves in this launch
+  uint32_t u_bits;   // random word of this step's Metropolis test
+  float pad;
+};
+static_assert(sizeof(LaneState) == 144, "LaneState layout");
+static_assert(sizeof(KItem) % 8 == 0, "KItem must keep the barriers 8-byte aligned");
+static_assert(TAB_BYTES % 16 == 0, "tile staging must start 16-byte aligned");
+
+size_t dock_smem_bytes(int A, int P, int NA, int n_stages) {
+  const int W = A * P;
   return (size_t)TAB_BYTES + (size_t)n_stages * STAGE_BYTES +
-         (size_t)n_warps * NRED * 32 * sizeof(double) + 32 * 36 * sizeof(float) +
-         (size_t)2 * n_stages * sizeof(uint64_t);
+         (size_t)W * NRED * 32 * sizeof(double) + (size_t)P * A * NA * 32 * sizeof(float) +
+         32 * sizeof(LaneState) + sizeof(KItem) + (size_t)2 * n_stages * sizeof(uint64_t);
+}
+
+// Hardware approximations (PTX rsqrt / rcp / ex2, flush-to-zero).
+__device__ __forceinline__ float frsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float frcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float fex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
 // Hydrophobic contact polynomial of calcenergy_d.cu:80-86 in Horner form:
@@ -51,72 +96,56 @@ __device__ __forceinline__ float hpc_poly(float d2) {
   return 1.0f - q * d2;
 }
 
-struct Rot {
-  float r00, r01, r02, r10, r11, r12, r20, r21, r22;
-};
-
-// Per-replica state in shared memory, written by warp 0 only.
-struct LaneState {
-  float m_old[6];
-  float m_new[6];
-  float rot[9];
-  float tr[3];
-  float e_old[GD_NTERM];
-  float pad[2];
-};
-
-// ZYX Euler rotation of move_d.cu:90-105.
-__device__ __forceinline__ Rot make_rot(float a3, float a4, float a5) {
+// ZYX Euler rotation of move_d.cu:90-105 (row-major 3x3).
+__device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R) {
   float s1, c1, s2, c2, s3, c3;
   sincosf(a3, &s1, &c1);
   sincosf(a4, &s2, &c2);
   sincosf(a5, &s3, &c3);
-  Rot R;
-  R.r00 = c1 * c2;
-  R.r01 = c1 * s2 * s3 - c3 * s1;
-  R.r02 = s1 * s3 + c1 * c3 * s2;
-  R.r10 = c2 * s1;
-  R.r11 = c1 * c3 + s1 * s2 * s3;
-  R.r12 = c3 * s1 * s2 - c1 * s3;
-  R.r20 = -1.0f * s2;
-  R.r21 = c2 * s3;
-  R.r22 = c2 * c3;
-  return R;
+  R[0] = c1 * c2;
+  R[1] = c1 * s2 * s3 - c3 * s1;
+  R[2] = s1 * s3 + c1 * c3 * s2;
+  R[3] = c2 * s1;
+  R[4] = c1 * c3 + s1 * s2 * s3;
+  R[5] = c3 * s1 * s2 - c1 * s3;
+  R[6] = -1.0f * s2;
+  R[7] = c2 * s3;
+  R[8] = c2 * c3;
 }
 
-template <int MODE>
+template <int MODE, int NA>
 __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
-    dock_kernel(const __grid_constant__ KTables T, const __grid_constant__ KRun R) {
+    dock_kernel(const __grid_constant__ KRun R) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int W = R.n_warps;
-  const int NS = R.n_stages;
+  const int A = R.A, P = R.P, W = A * P, NS = R.n_stages;
+  const int MAXA = A * NA;
   float4 *s_tab_a = reinterpret_cast<float4 *>(smem);
   float2 *s_tab_b = reinterpret_cast<float2 *>(smem + TAB_N * 16);
   unsigned char *s_tiles = smem + TAB_BYTES;
   double *s_red = reinterpret_cast<double *>(s_tiles + (size_t)NS * STAGE_BYTES);
-  LaneState *s_lane = reinterpret_cast<LaneState *>(s_red + (size_t)W * NRED * 32);
-  uint64_t *s_full = reinterpret_cast<uint64_t *>(s_lane + 32);
+  float *s_hpc = reinterpret_cast<float *>(s_red + (size_t)W * NRED * 32);
+  LaneState *s_lane = reinterpret_cast<LaneState *>(s_hpc + (size_t)P * MAXA * 32);
+  KItem *s_item = reinterpret_cast<KItem *>(s_lane + 32);
+  uint64_t *s_full = reinterpret_cast<uint64_t *>(s_item + 1);
   uint64_t *s_empty = s_full + NS;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
 
-  // ---- work of this CTA --------------------------------------------------
-  int rep0, n_act, prt_conf;
-  if (MODE == KMODE_POSES) {
-    rep0 = blockIdx.x * 32;
-    n_act = min(32, R.n_pose - rep0);
-    prt_conf = R.prt_conf;
-  } else {
-    rep0 = R.cta_rep0[blockIdx.x];
-    n_act = R.cta_nrep[blockIdx.x];
-    prt_conf = rep0 / (R.st.n_tmp * R.st.n_lig_conf);
+  // ---- item of this CTA into shared memory, type table, barriers ----------
+  const int item = (MODE == KMODE_POSES) ? 0 : R.cta_item[blockIdx.x];
+  const KItem &G = R.items[item];
+  {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&G);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(s_item);
+    for (int i = threadIdx.x; i < (int)(sizeof(KItem) / 4); i += blockDim.x) dst[i] = src[i];
+    const float4 *ta = G.T.tab_a;
+    const float2 *tb = G.T.tab_b;
+    for (int i = threadIdx.x; i < TAB_N; i += blockDim.x) {
+      s_tab_a[i] = ta[i];
+      s_tab_b[i] = tb[i];
+    }
   }
-  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
-  const bool resident = R.resident != 0;
-  const int n_steps = (MODE == KMODE_REMC) ? R.n_steps : 1;
-  const int passes = resident ? 1 : n_steps;
-
   if (threadIdx.x == 0) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(&s_full[i], 1);
@@ -124,13 +153,39 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     }
     fence_barrier_init();
   }
-  for (int i = threadIdx.x; i < TAB_N; i += blockDim.x) {
-    s_tab_a[i] = T.tab_a[i];
-    s_tab_b[i] = T.tab_b[i];
-  }
   __syncthreads();
+  const KItem &I = *s_item;
+  const KTables &T = I.T;
 
-  // ---- producer warp: streams the protein conformation -------------------
+  // ---- work of this CTA --------------------------------------------------
+  int rep0, n_act, prt_conf, lane_rep;
+  if (MODE == KMODE_POSES) {
+    rep0 = blockIdx.x * 32;
+    n_act = min(32, R.n_pose - rep0);
+    prt_conf = R.prt_conf;
+    lane_rep = rep0 + (lane < n_act ? lane : 0);
+  } else if (R.group_major) {
+    // whole exchange groups: lane = group offset * n_tmp + temperature slot
+    const int nt = I.n_tmp, nl = I.n_lig_conf;
+    const int g0 = R.cta_rep0[blockIdx.x];
+    n_act = R.cta_nrep[blockIdx.x];
+    rep0 = g0;
+    prt_conf = g0 / nl;
+    const int ln = lane < n_act ? lane : 0;
+    lane_rep = nt * nl * prt_conf + nl * (ln % nt) + (g0 % nl) + ln / nt;
+  } else {
+    rep0 = R.cta_rep0[blockIdx.x];
+    n_act = R.cta_nrep[blockIdx.x];
+    prt_conf = rep0 / (I.n_tmp * I.n_lig_conf);
+    lane_rep = rep0 + (lane < n_act ? lane : 0);
+  }
+  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  const bool resident = R.resident != 0;
+  const int n_steps = (MODE == KMODE_REMC) ? R.n_steps : 1;
+  const int passes = resident ? 1 : n_steps;
+  const int step_base = (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr : R.step0;
+
+  // ---- producer warp: stages the protein conformation -------------------
   if (warp == W) {
     if (lane == 0) {
       const float4 *src_a = T.pt_a + (size_t)prt_conf * T.pnp_pad;
@@ -154,30 +209,50 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   }
 
   // ---- compute warps -----------------------------------------------------
+  const int ag = warp % A, pg = warp / A;
   const int lna = T.lna;
   const bool active = lane < n_act;
-  const int rep = rep0 + (active ? lane : 0);
-  const int lig_conf = (MODE == KMODE_POSES) ? R.lig_conf : rep % R.st.n_lig_conf;
+  const int rep = lane_rep;                    // local replica / pose index
+  const int grep = I.rep_base + rep;           // replica in the state arrays
+  const int lig_conf = (MODE == KMODE_POSES) ? R.lig_conf : rep % I.n_lig_conf;
   const float4 *orig = T.lig + (size_t)lig_conf * lna;
   LaneState &me = s_lane[lane];
+  const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
 
-  // this warp's ligand atoms a = warp + W k
+  // this warp's atoms; padding atoms use the all-zero table row, no charge,
+  // and sit far from everything
+  int lto[NA];
+  float lq[NA], ox[NA], oy[NA], oz[NA];
   int n_my = 0;
 #pragma unroll
-  for (int k = 0; k < MAX_APW; ++k)
-    if (warp + W * k < lna) n_my = k + 1;
+  for (int k = 0; k < NA; ++k) {
+    const int a = ag + A * k;
+    if (a < lna) {
+      n_my = k + 1;
+      lto[k] = T.lig_t[a] * GD_NPT;
+      lq[k] = T.lig_q[a];
+      const float4 o = orig[a];
+      ox[k] = o.x;
+      oy[k] = o.y;
+      oz[k] = o.z;
+    } else {
+      lto[k] = GD_NLT * GD_NPT;
+      lq[k] = 0.f;
+      ox[k] = oy[k] = oz[k] = FAR;
+    }
+  }
 
-  // replica state lives in shared memory, owned by warp 0
-  float mbeta = 0.f;
-  int acs = 0, idx_tmp = 0;
   if (warp == 0) {
+    me.acs = 0;
+    me.idx_tmp = 0;
+    me.mbeta = 0.f;
     if (MODE == KMODE_REMC) {
-      idx_tmp = R.st.idx_tmp[rep];
-      mbeta = R.st.minus_beta[idx_tmp];
+      me.idx_tmp = R.idx_tmp[grep];
+      me.mbeta = I.minus_beta[me.idx_tmp];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) me.m_old[i] = R.st.m_old[(size_t)rep * 6 + i];
+      for (int i = 0; i < 6; ++i) me.m_old[i] = R.m_old[(size_t)grep * 6 + i];
 #pragma unroll
-      for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = R.st.e_old[(size_t)rep * GD_NTERM + i];
+      for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = R.e_old[(size_t)grep * GD_NTERM + i];
     } else {
 #pragma unroll
       for (int i = 0; i < 6; ++i) me.m_old[i] = 0.f;
@@ -185,69 +260,67 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = 0.f;
     }
   }
-  uint32_t k0 = 0, k1 = 0;
-  rng_key(R.seed, R.stream_id, k0, k1);
+  const float lj0 = T.lj0, lj0lj1 = T.lj0lj1, inv_el1 = T.inv_el1, near_d2 = T.near_d2;
 
-  int it = 0;  // tile iteration counter (streaming ring position)
+  int it = 0;  // streaming ring position
   for (int si = 0; si < n_steps; ++si) {
-    const int step = R.step0 + si;
+    const int step = step_base + si;
 
-    // ---- warp 0 proposes the move and publishes it ---------------------------
-    uint32_t u_acc_bits = 0;
+    // ---- warp 0 proposes the move and publishes it -------------------------
     if (warp == 0) {
       float m_new[6];
       if (MODE == KMODE_REMC) {
+        uint32_t k0, k1;
+        rng_key(I.seed, I.stream_id, k0, k1);
         const U4 a = philox4x32_10(U4{(uint32_t)rep, (uint32_t)step, 0u, 0u}, k0, k1);
         const U4 b = philox4x32_10(U4{(uint32_t)rep, (uint32_t)step, 1u, 0u}, k0, k1);
         const uint32_t bits[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
-        u_acc_bits = b.z;
+        me.u_bits = b.z;
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
           const float pert = __fadd_rn(__fmul_rn(2.0f, u01(bits[i])), -1.0f);
-          m_new[i] = __fadd_rn(__fmul_rn(R.move_scale[i], pert), me.m_old[i]);
+          m_new[i] = __fadd_rn(__fmul_rn(I.move_scale[i], pert), me.m_old[i]);
         }
       } else if (MODE == KMODE_INIT) {
-        const bool away = (R.flags & GD_MC_MOVE_AWAY) != 0;
+        const bool away = (I.flags & GD_MC_MOVE_AWAY) != 0;
 #pragma unroll
         for (int i = 0; i < 6; ++i)
-          m_new[i] = away ? __fadd_rn(__fmul_rn(R.move_scale[i], 44.5f), 0.0f) : 0.0f;
+          m_new[i] = away ? __fadd_rn(__fmul_rn(I.move_scale[i], 44.5f), 0.0f) : 0.0f;
       } else {
 #pragma unroll
         for (int i = 0; i < 6; ++i) m_new[i] = active ? R.poses[(size_t)rep * 6 + i] : 0.f;
       }
-      const Rot rot = make_rot(m_new[3], m_new[4], m_new[5]);
+      float rot[9];
+      make_rot(m_new[3], m_new[4], m_new[5], rot);
 #pragma unroll
       for (int i = 0; i < 6; ++i) me.m_new[i] = m_new[i];
-      me.rot[0] = rot.r00; me.rot[1] = rot.r01; me.rot[2] = rot.r02;
-      me.rot[3] = rot.r10; me.rot[4] = rot.r11; me.rot[5] = rot.r12;
-      me.rot[6] = rot.r20; me.rot[7] = rot.r21; me.rot[8] = rot.r22;
-      // translation applied after the rotation: m + ligand centre
-      me.tr[0] = m_new[0];
-      me.tr[1] = m_new[1];
-      me.tr[2] = m_new[2];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) me.rot[i] = rot[i];
     }
     named_sync(1, W * 32);
 
-    // ---- place this warp's atoms --------------------------------------------
+    // ---- place this warp's atoms -------------------------------------------
     const float q00 = me.rot[0], q01 = me.rot[1], q02 = me.rot[2];
     const float q10 = me.rot[3], q11 = me.rot[4], q12 = me.rot[5];
     const float q20 = me.rot[6], q21 = me.rot[7], q22 = me.rot[8];
-    const float t0 = me.tr[0], t1 = me.tr[1], t2 = me.tr[2];
-    float lx[MAX_APW], ly[MAX_APW], lz[MAX_APW], hpc[MAX_APW];
+    const float t0 = me.m_new[0], t1 = me.m_new[1], t2 = me.m_new[2];
+    float lx[NA], ly[NA], lz[NA];
+    // per-atom hydrophobic sums of this warp's tiles live in shared memory
+    // (touched only on the close-range path)
+    float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per atom
 #pragma unroll
-    for (int k = 0; k < MAX_APW; ++k) {
-      lx[k] = ly[k] = lz[k] = hpc[k] = 0.f;
-      if (k < n_my) {
-        const float4 o = orig[warp + W * k];
-        lx[k] = q00 * o.x + q01 * o.y + q02 * o.z + t0 + T.lig_center[0];
-        ly[k] = q10 * o.x + q11 * o.y + q12 * o.z + t1 + T.lig_center[1];
-        lz[k] = q20 * o.x + q21 * o.y + q22 * o.z + t2 + T.lig_center[2];
-      }
+    for (int k = 0; k < NA; ++k) {
+      lx[k] = q00 * ox[k] + q01 * oy[k] + q02 * oz[k] + t0 + lcx;
+      ly[k] = q10 * ox[k] + q11 * oy[k] + q12 * oz[k] + t1 + lcy;
+      lz[k] = q20 * ox[k] + q21 * oy[k] + q22 * oz[k] + t2 + lcz;
+      if (k < n_my) my_hpc[(size_t)A * k * 32] = 0.f;
     }
 
     // ---- pair terms over the protein tiles -----------------------------------
     double dvdw = 0.0, dele = 0.0, dpmf = 0.0, dpsp = 0.0, dhdb = 0.0;
-    for (int t = 0; t < n_tiles; ++t, ++it) {
+    const int t_first = resident ? pg : 0;
+    const int t_step = resident ? P : 1;
+    for (int t = t_first; t < n_tiles; t += t_step, ++it) {
       const int s = resident ? t : (it % NS);
       const uint32_t ph = resident ? 0u : (uint32_t)((it / NS) & 1);
       mbar_wait(&s_full[s], ph, R.err, 2);
@@ -259,58 +332,68 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
         const int j1 = min(nvalid, j0 + CHUNK);
         float fvdw = 0.f, fele = 0.f, fpmf = 0.f, fpsp = 0.f, fhdb = 0.f;
         for (int j = j0; j < j1; ++j) {
-          const float4 A = ta[j];
-          const float2 B = tb[j];
-          const uint32_t meta = __float_as_uint(B.y);
+          const float4 Ap = ta[j];
+          const float2 Bp = tb[j];
+          const uint32_t meta = __float_as_uint(Bp.y);
           const int pt = (int)(meta & META_TYPE_MASK);
-          const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
-          const bool hflag = (meta & META_HPC_BIT) != 0u;
+          float d2v[NA], rv[NA];
+          float mn = 3.0e38f;
+          // fast path: soft LJ, far-field electrostatics, contact PMF
 #pragma unroll
-          for (int k = 0; k < MAX_APW; ++k) {
-            if (k < n_my) {
-              const int lt = T.lig_t[warp + W * k];
-              const float4 P = s_tab_a[lt * GD_NPT + pt];  // p1a p2a pmf0 pmf1
-              const float2 H = s_tab_b[lt * GD_NPT + pt];  // hdb0 hdb1
-              const float dx = lx[k] - A.x;
-              const float dy = ly[k] - A.y;
-              const float dz = lz[k] - A.z;
-              const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-              const float r = rsqrtf(d2);
-              const float d = d2 * r;
-              // hydrophobic contact (per ligand atom)
-              if (hflag) {
-                if (d2 <= 81.0f) hpc[k] = fmaf(B.x, hpc_poly(d2), hpc[k]);
+          for (int k = 0; k < NA; ++k) {
+            const float4 Pk = s_tab_a[lto[k] + pt];  // p1a p2a pmf0 pmf1
+            const float dx = lx[k] - Ap.x;
+            const float dy = ly[k] - Ap.y;
+            const float dz = lz[k] - Ap.z;
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float r = frsqrt(d2);
+            const float d = d2 * r;
+            const float r2 = r * r;
+            const float r6 = r2 * r2 * r2;
+            const float r9 = r6 * r2 * r;
+            const float p1 = Pk.x * r9;
+            const float p2 = Pk.y * r6;
+            const float p4 = fmaf(p1, fmaf(lj0lj1, d2, lj0), 1.0f);
+            fvdw = fmaf(p1 - p2, frcp(p4), fvdw);
+            fele = fmaf(lq[k] * Ap.w, r * inv_el1, fele);
+            const float dm = d - Pk.z;
+            const float ex = fex2(fmaf(-0.5f * LOG2E, d, 6.0f * LOG2E) * dm);
+            fpmf = fmaf(Pk.w, frcp(1.0f + ex), fpmf);
+            d2v[k] = d2;
+            rv[k] = r;
+            mn = fminf(mn, d2);
+          }
+          // hydrogen bond, for the type pairs that define one
+#pragma unroll
+          for (int k = 0; k < NA; ++k) {
+            const float2 Hk = s_tab_b[lto[k] + pt];  // hdb0 hdb1
+            if (Hk.x > 0.1f) {
+              const float h3 = (d2v[k] * rv[k] - Hk.x) * Hk.y;
+              fhdb = fmaf(Hk.y, fex2((-0.5f * LOG2E) * h3 * h3), fhdb);
+            }
+          }
+          // close-range terms, only when some lane has an atom within near_d2
+          if (__any_sync(0xffffffffu, mn <= near_d2)) {
+            const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
+            const bool hflag = (meta & META_HPC_BIT) != 0u;
+#pragma unroll
+            for (int k = 0; k < NA; ++k) {
+              const float d2 = d2v[k];
+              const float d = d2 * rv[k];
+              if (hflag && d2 <= 81.0f && k < n_my) {
+                float *h = my_hpc + (size_t)A * k * 32;
+                *h = fmaf(Bp.x, hpc_poly(d2), *h);
               }
-              // soft Lennard-Jones: p1 = p1a/d^9, p2 = p2a/d^6
-              const float r2 = r * r;
-              const float r6 = r2 * r2 * r2;
-              const float r9 = r6 * r2 * r;
-              const float p1 = P.x * r9;
-              const float p2 = P.y * r6;
-              const float p4 = fmaf(p1, fmaf(T.lj0lj1, d2, T.lj0), 1.0f);
-              fvdw += __fdividef(p1 - p2, p4);
-              // soft electrostatics
               const float s1 = T.el1 * d;
-              const float g = (s1 < 1.0f) ? fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0)
-                                          : r * T.inv_el1;
-              fele = fmaf(T.lig_q[warp + W * k] * A.w, g, fele);
-              // contact PMF
-              const float dm = d - P.z;
-              const float ex = __expf(fmaf(-0.5f, d, 6.0f) * dm);
-              fpmf += __fdividef(P.w, 1.0f + ex);
-              // pocket-specific potential
-              if (is_c2) {
-                const bool hit = dm <= 0.0f;
-                if (__any_sync(0xffffffffu, hit)) {
-                  const float v =
-                      __ldg(&T.psp[(size_t)lt * T.psp_ncol + (meta >> META_SEQ_SHIFT)]);
-                  if (hit) fpsp += v;
-                }
+              if (s1 < 1.0f) {
+                const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
+                fele = fmaf(lq[k] * Ap.w, gnear - rv[k] * inv_el1, fele);
               }
-              // hydrogen bond
-              if (H.x > 0.1f) {
-                const float h3 = (d - H.x) * H.y;
-                fhdb = fmaf(H.y, __expf(-0.5f * h3 * h3), fhdb);
+              if (is_c2 && k < n_my) {
+                const float dm = d - s_tab_a[lto[k] + pt].z;
+                if (dm <= 0.0f)
+                  fpsp += __ldg(&T.psp[(size_t)(lto[k] / GD_NPT) * T.psp_ncol +
+                                       (meta >> META_SEQ_SHIFT)]);
               }
             }
           }
@@ -327,23 +410,23 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       }
     }
 
-    // ---- hydrophobic restraint per atom, KDE --------------------------------
-    double dhpc = 0.0, dkde = 0.0, dlhm = 0.0;
+    // ---- per-atom hydrophobic sums, KDE --------------------------------------
+    double dkde = 0.0, dlhm = 0.0;
 #pragma unroll
-    for (int k = 0; k < MAX_APW; ++k) {
+    for (int k = 0; k < NA; ++k) {
       if (k < n_my) {
-        const int lt = T.lig_t[warp + W * k];
-        const float h = __fdiv_rn(__fsub_rn(hpc[k], T.hpl0[lt]), T.hpl1[lt]);
-        dhpc += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, h), h), T.hpl2[lt]);
-        const int kb = T.kde_off[lt], ke = T.kde_off[lt + 1];
-        if (ke > kb) {
-          float kv = 0.f;
-          for (int q = kb; q < ke; ++q) {
-            const float4 K = T.kde[q];
-            const float dx = lx[k] - K.x, dy = ly[k] - K.y, dz = lz[k] - K.z;
-            kv += __expf(T.kde2 * fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+        if (k % P == pg) {
+          const int lt = lto[k] / GD_NPT;
+          const int kb = T.kde_off[lt], ke = T.kde_off[lt + 1];
+          if (ke > kb) {
+            float kv = 0.f;
+            for (int q = kb; q < ke; ++q) {
+              const float4 K = T.kde[q];
+              const float dx = lx[k] - K.x, dy = ly[k] - K.y, dz = lz[k] - K.z;
+              kv += fex2(T.kde2 * LOG2E * fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+            }
+            dkde += (double)kv / (double)(ke - kb);
           }
-          dkde += (double)kv / (double)(ke - kb);
         }
       }
     }
@@ -355,9 +438,9 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
         const float4 M = Mm[l];
         if (M.w != 0.0f) {
           const float4 o = orig[l];
-          const float x = q00 * o.x + q01 * o.y + q02 * o.z + t0 + T.lig_center[0];
-          const float y = q10 * o.x + q11 * o.y + q12 * o.z + t1 + T.lig_center[1];
-          const float z = q20 * o.x + q21 * o.y + q22 * o.z + t2 + T.lig_center[2];
+          const float x = q00 * o.x + q01 * o.y + q02 * o.z + t0 + lcx;
+          const float y = q10 * o.x + q11 * o.y + q12 * o.z + t1 + lcy;
+          const float z = q20 * o.x + q21 * o.y + q22 * o.z + t2 + lcz;
           const float dx = x - M.x, dy = y - M.y, dz = z - M.z;
           sv += fmaf(dz, dz, fmaf(dy, dy, dx * dx));
         }
@@ -373,7 +456,7 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       red[2 * 32 + lane] = dpmf;
       red[3 * 32 + lane] = dpsp;
       red[4 * 32 + lane] = dhdb;
-      red[5 * 32 + lane] = dhpc;
+      red[5 * 32 + lane] = 0.0;
       red[6 * 32 + lane] = dkde;
       red[7 * 32 + lane] = dlhm;
     }
@@ -387,6 +470,14 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
 #pragma unroll
         for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
       }
+      // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149)
+      for (int a = 0; a < lna; ++a) {
+        float h = 0.f;
+        for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
+        const int lt = T.lig_t[a];
+        const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
+        S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
+      }
       const double n = (double)lna;
       double raw[GD_NRAW];
       raw[0] = S[0] / n;
@@ -399,9 +490,9 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       raw[7] = log(S[7] / (double)T.pos);
       {
         // distance to the pocket (calcenergy_d.cu:278-283); centre = c + m
-        const float cx = __fadd_rn(T.lig_center[0], me.m_new[0]);
-        const float cy = __fadd_rn(T.lig_center[1], me.m_new[1]);
-        const float cz = __fadd_rn(T.lig_center[2], me.m_new[2]);
+        const float cx = __fadd_rn(lcx, me.m_new[0]);
+        const float cy = __fadd_rn(lcy, me.m_new[1]);
+        const float cz = __fadd_rn(lcz, me.m_new[2]);
         const float dx = __fsub_rn(cx, T.pocket[0]);
         const float dy = __fsub_rn(cy, T.pocket[1]);
         const float dz = __fsub_rn(cz, T.pocket[2]);
@@ -431,14 +522,13 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
         if (MODE == KMODE_INIT) {
           acc = 1;  // forced accept with beta = 0 (montecarlo_d.cu:236-239)
         } else {
-          acc = metropolis(e[9], me.e_old[9], mbeta, u01(u_acc_bits));
-          if (active && R.st.record && step < R.st.rec_steps) {
-            gd_record *rc = R.st.record + (size_t)rep * R.st.rec_steps + step;
-            const int nl = R.st.n_lig_conf, nt = R.st.n_tmp;
+          acc = metropolis(e[9], me.e_old[9], me.mbeta, u01(me.u_bits));
+          if (active && I.record && step < I.rec_steps) {
+            gd_record *rc = I.record + (size_t)rep * I.rec_steps + step;
             rc->idx_rep = rep;
-            rc->idx_prt = rep / (nt * nl);
-            rc->idx_tmp = idx_tmp;
-            rc->idx_lig = rep % nl;
+            rc->idx_prt = prt_conf;
+            rc->idx_tmp = me.idx_tmp;
+            rc->idx_lig = lig_conf;
 #pragma unroll
             for (int i = 0; i < GD_NTERM; ++i) rc->e[i] = me.e_old[i];
             rc->cmcc = 0.f;
@@ -450,72 +540,129 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
           }
         }
         if (acc) {
-          acs += 1;
+          me.acs += 1;
 #pragma unroll
           for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = e[i];
 #pragma unroll
           for (int i = 0; i < 6; ++i) me.m_old[i] = me.m_new[i];
         }
+        // temperature exchange of the CTA's own groups at the end of every
+        // interval (exchangereplicas_d.cu:26-79); slot t of group gi is lane
+        // gi * n_tmp + t, so the groups never leave the CTA
+        if (MODE == KMODE_REMC && R.fused_exchange && ((step + 1) % R.spe) == 0 &&
+            (I.flags & GD_MC_EXCHANGE)) {
+          const int nt = I.n_tmp;
+          int *s_tmp = reinterpret_cast<int *>(s_red);          // 32 ints
+          float *s_en = reinterpret_cast<float *>(s_red) + 32;  // 32 floats
+          s_tmp[lane] = me.idx_tmp;
+          s_en[lane] = me.e_old[GD_E_TOTAL];
+          __syncwarp();
+          const int s0 = step + 1 - R.spe;
+          const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
+          const int mode_t = (within / R.spe) % 2;
+          if (active && (lane % nt) == 0) {
+            const int b = lane;  // first slot of this group
+            const uint32_t gid = (uint32_t)(prt_conf * I.n_lig_conf + (rep % I.n_lig_conf));
+            uint32_t k0, k1;
+            rng_key(I.seed, I.stream_id, k0, k1);
+            int orders[MAX_TMP];
+            for (int t = 0; t < nt; ++t) orders[s_tmp[b + t]] = t;
+            const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
+            for (int pair = 0; pair < maxpair; ++pair) {
+              const int i1 = (pair << 1) + mode_t;
+              const int o1 = orders[i1], o2 = orders[i1 + 1];
+              const int tt = s_tmp[b + o1];
+              const float mb1 = I.minus_beta[s_tmp[b + o1]];
+              const float mb2 = I.minus_beta[s_tmp[b + o2]];
+              const float delta =
+                  __fmul_rn(__fsub_rn(mb1, mb2), __fsub_rn(s_en[b + o2], s_en[b + o1]));
+              const float prob = decision_expf(delta);
+              const U4 o =
+                  philox4x32_10(U4{gid, (uint32_t)(s0 / R.spe), 2u, (uint32_t)pair}, k0, k1);
+              if (prob > u01(o.x)) {
+                s_tmp[b + o1] = s_tmp[b + o2];
+                s_tmp[b + o2] = tt;
+                atomicAdd(&I.acs_exchg[o1], 1);
+                atomicAdd(&I.acs_exchg[o2], 1);
+              }
+            }
+          }
+          __syncwarp();
+          me.idx_tmp = s_tmp[lane];
+          me.mbeta = I.minus_beta[me.idx_tmp];
+        }
       }
     }
-    // the next iteration's first barrier orders warp 0's updates before any
-    // other warp reads the lane state again
+    // the next step's first barrier orders warp 0's updates (and its use of
+    // s_red for the exchange) before any other warp touches them again
   }
 
   // ---- write the replica state back ----------------------------------------
   if (MODE != KMODE_POSES && warp == 0 && active) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i) R.st.m_old[(size_t)rep * 6 + i] = me.m_old[i];
+    for (int i = 0; i < 6; ++i) R.m_old[(size_t)grep * 6 + i] = me.m_old[i];
 #pragma unroll
-    for (int i = 0; i < GD_NTERM; ++i) R.st.e_old[(size_t)rep * GD_NTERM + i] = me.e_old[i];
+    for (int i = 0; i < GD_NTERM; ++i) R.e_old[(size_t)grep * GD_NTERM + i] = me.e_old[i];
     if (MODE == KMODE_INIT) {
-      R.st.acs_mc[rep] = 0;
-      R.st.idx_tmp[rep] = (rep / R.st.n_lig_conf) % R.st.n_tmp;
+      R.acs_mc[grep] = 0;
+      R.idx_tmp[grep] = (rep / I.n_lig_conf) % I.n_tmp;
     } else {
-      R.st.acs_mc[rep] += acs;
+      R.acs_mc[grep] += me.acs;
+      if (R.fused_exchange) R.idx_tmp[grep] = me.idx_tmp;
     }
   }
 }
 
-// Temperature exchange, one thread per (protein conf, ligand conf) group
-// (exchangereplicas_d.cu:26-79).  Pairs of adjacent temperature indices
-// (2 pair + mode_t, 2 pair + mode_t + 1) swap their slots when
+// Temperature exchange, one thread per (item, protein conf, ligand conf)
+// group (exchangereplicas_d.cu:26-79).  Pairs of adjacent temperature
+// indices (2 pair + mode_t, 2 pair + mode_t + 1) swap their slots when
 // exp((mb1 - mb2)(E2 - E1)) > u; the counters are kept per slot.
-__global__ void exchange_kernel(KState S, int n_prt, int n_lig, uint64_t seed, uint32_t stream,
-                                int round, int mode_t) {
+__global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_groups,
+                                const float *e_old, int *idx_tmp_g, int spe, int step0,
+                                const int *step_ptr) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_prt * n_lig) return;
-  const int p = g / n_lig, l = g % n_lig;
-  const int nt = S.n_tmp;
+  if (g >= n_groups) return;
+  const KGroup G = groups[g];
+  const KItem &I = items[G.item];
+  const int s0 = step_ptr ? *step_ptr : step0;
+  const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
+  const int mode_t = (within / spe) % 2;
+  const int round = s0 / spe;
+  const int nt = I.n_tmp, nl = I.n_lig_conf;
   int temps[MAX_TMP], orders[MAX_TMP];
   float en[MAX_TMP];
   for (int t = 0; t < nt; ++t) {
-    const int r = nt * n_lig * p + n_lig * t + l;
-    temps[t] = S.idx_tmp[r];
-    en[t] = S.e_old[(size_t)r * GD_NTERM + GD_E_TOTAL];
+    const int r = I.rep_base + nt * nl * G.p + nl * t + G.l;
+    temps[t] = idx_tmp_g[r];
+    en[t] = e_old[(size_t)r * GD_NTERM + GD_E_TOTAL];
   }
   for (int t = 0; t < nt; ++t) orders[temps[t]] = t;
   uint32_t k0, k1;
-  rng_key(seed, stream, k0, k1);
+  rng_key(I.seed, I.stream_id, k0, k1);
+  const uint32_t gid = (uint32_t)(G.p * nl + G.l);
   const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
   for (int pair = 0; pair < maxpair; ++pair) {
     const int i1 = (pair << 1) + mode_t;
     const int i2 = i1 + 1;
     const int o1 = orders[i1], o2 = orders[i2];
     const int tt = temps[o1];
-    const float mb1 = S.minus_beta[temps[o1]];
-    const float mb2 = S.minus_beta[temps[o2]];
+    const float mb1 = I.minus_beta[temps[o1]];
+    const float mb2 = I.minus_beta[temps[o2]];
     const float delta = __fmul_rn(__fsub_rn(mb1, mb2), __fsub_rn(en[o2], en[o1]));
     const float prob = decision_expf(delta);
-    const U4 o = philox4x32_10(U4{(uint32_t)g, (uint32_t)round, 2u, (uint32_t)pair}, k0, k1);
+    const U4 o = philox4x32_10(U4{gid, (uint32_t)round, 2u, (uint32_t)pair}, k0, k1);
     if (prob > u01(o.x)) {
       temps[o1] = temps[o2];
       temps[o2] = tt;
-      atomicAdd(&S.acs_exchg[o1], 1);
-      atomicAdd(&S.acs_exchg[o2], 1);
+      atomicAdd(&I.acs_exchg[o1], 1);
+      atomicAdd(&I.acs_exchg[o2], 1);
     }
   }
-  for (int t = 0; t < nt; ++t) S.idx_tmp[nt * n_lig * p + n_lig * t + l] = temps[t];
+  for (int t = 0; t < nt; ++t) idx_tmp_g[I.rep_base + nt * nl * G.p + nl * t + G.l] = temps[t];
+}
+
+__global__ void advance_kernel(int *step_ptr, int spe) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *step_ptr += spe;
 }
 
 __global__ void metropolis_kernel(int n, const float *e_new, const float *e_old,
@@ -568,37 +715,52 @@ __global__ void fma_peak_kernel(float *out, int iters) {
 }
 
 // ---------------------------------------------------------------------------
-cudaError_t launch_dock(const KTables &T, const KRun &R, int grid, cudaStream_t s) {
-  const size_t smem = dock_smem_bytes(R.n_warps, R.n_stages);
-  const int threads = (R.n_warps + 1) * 32;
-  cudaError_t e;
-  switch (R.mode) {
-    case KMODE_POSES:
-      e = cudaFuncSetAttribute(dock_kernel<KMODE_POSES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if (e != cudaSuccess) return e;
-      dock_kernel<KMODE_POSES><<<grid, threads, smem, s>>>(T, R);
-      break;
-    case KMODE_REMC:
-      e = cudaFuncSetAttribute(dock_kernel<KMODE_REMC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if (e != cudaSuccess) return e;
-      dock_kernel<KMODE_REMC><<<grid, threads, smem, s>>>(T, R);
-      break;
-    default:
-      e = cudaFuncSetAttribute(dock_kernel<KMODE_INIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if (e != cudaSuccess) return e;
-      dock_kernel<KMODE_INIT><<<grid, threads, smem, s>>>(T, R);
-      break;
-  }
+template <int MODE, int NA>
+static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
+  const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages);
+  const int threads = (R.A * R.P + 1) * 32;
+  cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dock_kernel<MODE, NA><<<grid, threads, smem, s>>>(R);
   return cudaGetLastError();
 }
 
-cudaError_t launch_exchange(const KState &S, int n_prt, int n_lig, uint64_t seed,
-                            uint32_t stream_id, int round, int mode_t, cudaStream_t s) {
-  const int n = n_prt * n_lig;
-  exchange_kernel<<<(n + 127) / 128, 128, 0, s>>>(S, n_prt, n_lig, seed, stream_id, round, mode_t);
+template <int MODE>
+static cudaError_t launch_mode(const KRun &R, int NA, int grid, cudaStream_t s) {
+  switch (NA) {
+    case 1: return launch_na<MODE, 1>(R, grid, s);
+    case 2: return launch_na<MODE, 2>(R, grid, s);
+    case 3: return launch_na<MODE, 3>(R, grid, s);
+    case 4: return launch_na<MODE, 4>(R, grid, s);
+    case 5: return launch_na<MODE, 5>(R, grid, s);
+    case 6: return launch_na<MODE, 6>(R, grid, s);
+    case 8: return launch_na<MODE, 8>(R, grid, s);
+    case 10: return launch_na<MODE, 10>(R, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
+  switch (R.mode) {
+    case KMODE_POSES: return launch_mode<KMODE_POSES>(R, NA, grid, s);
+    case KMODE_REMC: return launch_mode<KMODE_REMC>(R, NA, grid, s);
+    default: return launch_mode<KMODE_INIT>(R, NA, grid, s);
+  }
+}
+
+cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups,
+                            const float *e_old, int *idx_tmp, int spe, int step0,
+                            const int *step_ptr, cudaStream_t s) {
+  if (n_groups <= 0) return cudaSuccess;
+  exchange_kernel<<<(n_groups + 127) / 128, 128, 0, s>>>(items, groups, n_groups, e_old,
+                                                          idx_tmp, spe, step0, step_ptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance(int *step_ptr, int spe, cudaStream_t s) {
+  advance_kernel<<<1, 32, 0, s>>>(step_ptr, spe);
   return cudaGetLastError();
 }
 

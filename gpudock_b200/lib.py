@@ -38,6 +38,20 @@ def _declare(lib):
         "gd_ctx_sync": ([P], i32),
         "gd_ctx_launch_count": ([P], u64),
         "gd_complex_upload": ([P, C.POINTER(abi.GdComplex), C.POINTER(P)], i32),
+        "gd_complex_upload_shared": ([P, C.POINTER(abi.GdComplex), P, i32, i32, C.POINTER(P)],
+                                     i32),
+        "gd_autotune": ([P, P, C.POINTER(abi.GdTile), C.POINTER(C.c_double)], i32),
+        "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
+        "gd_batch_create": ([P, i32, C.POINTER(P), C.POINTER(abi.GdMcParams), C.POINTER(P)], i32),
+        "gd_batch_init": ([P], i32),
+        "gd_batch_run": ([P, i32], i32),
+        "gd_batch_read": ([P, i32, C.POINTER(abi.GdMcLog)], i32),
+        "gd_batch_destroy": ([P], i32),
+        "gd_batch_n_rep": ([P], i32),
+        "gd_batch_n_launch_shapes": ([P], i32),
+        "gd_batch_set_profiling": ([P, i32], i32),
+        "gd_batch_kernel_times": ([P, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int)], i32),
         "gd_complex_free": ([P], i32),
         "gd_complex_device_bytes": ([P], C.c_size_t),
         "gd_energy_poses_dev": ([P, P, i32, i32, i32, P, P, P], i32),
@@ -148,15 +162,35 @@ class Context:
 
 
 class DeviceComplex:
-    """A complex uploaded to the device in the kernel layout (gd_dcomplex)."""
+    """A complex uploaded to the device in the kernel layout (gd_dcomplex).
 
-    def __init__(self, ctx: Context, cx: abi.Complex):
+    With ``share`` the protein arrays of that uploaded complex are reused
+    (conformations ``prt_conf0 .. prt_conf0 + n_prt - 1``) instead of copied.
+    """
+
+    def __init__(self, ctx: Context, cx: abi.Complex, share: "DeviceComplex | None" = None,
+                 prt_conf0: int = 0, n_prt: int = 1):
         self.ctx = ctx
         self.cx = cx
+        self.share = share
         h = C.c_void_p()
-        check(ctx._lib.gd_complex_upload(ctx.h, C.byref(cx.struct()), C.byref(h)),
-              "gd_complex_upload")
+        self.n_prt_view = cx.n_prt if share is None else n_prt
+        if share is None:
+            check(ctx._lib.gd_complex_upload(ctx.h, C.byref(cx.struct()), C.byref(h)),
+                  "gd_complex_upload")
+        else:
+            check(ctx._lib.gd_complex_upload_shared(ctx.h, C.byref(cx.struct()), share.h,
+                                                    prt_conf0, n_prt, C.byref(h)),
+                  "gd_complex_upload_shared")
         self.h = h
+
+    def autotune(self):
+        """Autotunes the launch shape of this complex's size class."""
+        t = abi.GdTile()
+        ms = C.c_double()
+        check(self.ctx._lib.gd_autotune(self.ctx.h, self.h, C.byref(t), C.byref(ms)),
+              "gd_autotune")
+        return (t.atom_groups, t.tile_groups, t.atoms_per_warp), ms.value
 
     @property
     def device_bytes(self) -> int:
@@ -238,6 +272,63 @@ class Remc:
     def close(self):
         if self.h:
             self.dcx.ctx._lib.gd_remc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many complexes advanced together (gd_batch): the batched form."""
+
+    def __init__(self, ctx: Context, dcxs, params):
+        self.ctx = ctx
+        self.dcxs = list(dcxs)
+        self.params = [p for p, _ in params]
+        self._keep = [k for _, k in params]
+        n = len(self.dcxs)
+        arr = (C.c_void_p * n)(*[d.h.value for d in self.dcxs])
+        parr = (abi.GdMcParams * n)(*self.params)
+        h = C.c_void_p()
+        check(ctx._lib.gd_batch_create(ctx.h, n, C.cast(arr, C.POINTER(C.c_void_p)), parr,
+                                       C.byref(h)), "gd_batch_create")
+        self.h = h
+        self.n_rep = int(ctx._lib.gd_batch_n_rep(h))
+        self.n_shapes = int(ctx._lib.gd_batch_n_launch_shapes(h))
+
+    def init(self):
+        check(self.ctx._lib.gd_batch_init(self.h), "gd_batch_init")
+
+    def run(self, n_steps: int):
+        check(self.ctx._lib.gd_batch_run(self.h, int(n_steps)), "gd_batch_run")
+
+    def read(self, i: int) -> abi.McLogBuffers:
+        p = self.params[i]
+        n_rep = self._n_rep_of(i)
+        buf = abi.McLogBuffers(n_rep, p.n_tmp, p.steps_total, bool(p.flags & abi.MC_RECORD))
+        check(self.ctx._lib.gd_batch_read(self.h, i, C.byref(buf.log)), "gd_batch_read")
+        return buf
+
+    def _n_rep_of(self, i):
+        d = self.dcxs[i]
+        return d.n_prt_view * d.cx.n_lig * self.params[i].n_tmp
+
+    def set_profiling(self, on: bool = True):
+        check(self.ctx._lib.gd_batch_set_profiling(self.h, int(on)), "gd_batch_set_profiling")
+
+    def kernel_times(self):
+        a, b = C.c_double(), C.c_double()
+        na, nb = C.c_int(), C.c_int()
+        check(self.ctx._lib.gd_batch_kernel_times(self.h, C.byref(a), C.byref(na), C.byref(b),
+                                                  C.byref(nb)), "gd_batch_kernel_times")
+        return a.value, na.value, b.value, nb.value
+
+    def close(self):
+        if self.h:
+            self.ctx._lib.gd_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

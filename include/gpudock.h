@@ -215,9 +215,36 @@ uint64_t gd_ctx_launch_count(const gd_ctx *ctx);
  * ligand atom).  Replaces the table staging of run.cu:114-256. */
 gd_status gd_complex_upload(gd_ctx *ctx, const gd_complex *cx,
                             gd_dcomplex **out);
+/* Like gd_complex_upload, but the protein arrays are not copied: the new
+ * complex reads conformations [prt_conf0, prt_conf0 + n_prt) of `protein`
+ * (an uploaded complex of the same protein, kept alive by the new handle).
+ * Used to batch many ligands against one resident protein. */
+gd_status gd_complex_upload_shared(gd_ctx *ctx, const gd_complex *cx,
+                                   const gd_dcomplex *protein, int prt_conf0,
+                                   int n_prt, gd_dcomplex **out);
 gd_status gd_complex_free(gd_dcomplex *dcx);
 /* Device bytes held by an uploaded complex. */
 size_t gd_complex_device_bytes(const gd_dcomplex *dcx);
+
+/* ------------------------------------------------------------------------ */
+/* Launch shape of the energy kernel and its autotuner                      */
+/* ------------------------------------------------------------------------ */
+/* The compute warps of a CTA form an atom_groups x tile_groups grid; each
+ * warp keeps atoms_per_warp ligand atoms in registers and sweeps every
+ * tile_groups-th protein tile. */
+typedef struct gd_tile {
+  int atom_groups;
+  int tile_groups;
+  int atoms_per_warp;
+} gd_tile;
+
+/* Times every compiled launch shape for this complex's size class (ligand
+ * atoms, protein tiles) on one wave of pose CTAs, keeps the fastest in the
+ * context and returns it; later launches of that size class use it. */
+gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *dcx, gd_tile *best,
+                      double *best_ms);
+/* Sets the launch shape of a size class explicitly. */
+gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile);
 
 /* ------------------------------------------------------------------------ */
 /* Pose energies (CalcEnergy_d after Move_d on a given move vector)         */
@@ -310,6 +337,29 @@ gd_status gd_remc_kernel_times(gd_remc *remc, double *mc_ms, int *mc_launches,
  * free.  The counterpart of Run (run.cu:41-353). */
 gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc,
                  gd_mc_log *log);
+
+/* ------------------------------------------------------------------------ */
+/* Batched form: many complexes of uneven sizes advanced together.  All     */
+/* share steps_per_exchange; each keeps its own replicas, temperatures,     */
+/* random stream and counters.  Complexes with the same launch shape share  */
+/* one launch; with whole exchange groups per CTA (32 % n_tmp == 0) the     */
+/* exchange runs inside the kernel and a run is one launch per shape,       */
+/* otherwise the interval sequence is replayed from a captured CUDA graph.  */
+/* ------------------------------------------------------------------------ */
+typedef struct gd_batch gd_batch;
+
+gd_status gd_batch_create(gd_ctx *ctx, int n, const gd_dcomplex *const *items,
+                          const gd_mc_params *params, gd_batch **out);
+gd_status gd_batch_init(gd_batch *batch);
+gd_status gd_batch_run(gd_batch *batch, int n_steps);
+/* Results of complex `item` (same layout as gd_remc_read). */
+gd_status gd_batch_read(gd_batch *batch, int item, gd_mc_log *log);
+gd_status gd_batch_destroy(gd_batch *batch);
+int gd_batch_n_rep(const gd_batch *batch);
+int gd_batch_n_launch_shapes(const gd_batch *batch);
+gd_status gd_batch_set_profiling(gd_batch *batch, int on);
+gd_status gd_batch_kernel_times(gd_batch *batch, double *mc_ms, int *mc_launches,
+                                double *exch_ms, int *exch_launches);
 
 /* ------------------------------------------------------------------------ */
 /* Building blocks exposed for testing: the Metropolis and exchange rules   */
