@@ -119,6 +119,14 @@ class GdTile(C.Structure):
     _fields_ = [("atom_groups", C.c_int), ("tile_groups", C.c_int), ("atoms_per_warp", C.c_int)]
 
 
+class GdServerStats(C.Structure):
+    _fields_ = [
+        ("queued", C.c_int), ("active", C.c_int), ("completed", C.c_uint64),
+        ("iterations", C.c_uint64), ("launches", C.c_uint64), ("bytes_in_use", C.c_size_t),
+        ("busy_s", C.c_double),
+    ]
+
+
 class GdMcParams(C.Structure):
     _fields_ = [
         ("steps_total", C.c_int), ("steps_per_exchange", C.c_int),

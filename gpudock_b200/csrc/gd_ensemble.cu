@@ -168,6 +168,10 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     KItem &I = E.items[i];
     I.minus_beta = E.minus_beta + (size_t)i * MAX_TMP;
     I.acs_exchg = E.acs_exchg + (size_t)i * MAX_TMP;
+    I.m_old = E.m_old + (size_t)I.rep_base * 6;
+    I.e_old = E.e_old + (size_t)I.rep_base * GD_NTERM;
+    I.idx_tmp = E.idx_tmp + I.rep_base;
+    I.acs_mc = E.acs_mc + I.rep_base;
     I.record = nullptr;
     if (mc[i].flags & GD_MC_RECORD) {
       gd_record *rec = nullptr;
@@ -257,10 +261,6 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   R.group_major = pl.group_major;
   R.fused_exchange = pl.fused;
   R.spe = E.spe;
-  R.m_old = E.m_old;
-  R.e_old = E.e_old;
-  R.idx_tmp = E.idx_tmp;
-  R.acs_mc = E.acs_mc;
   R.err = E.ctx->d_err;
   return R;
 }
@@ -326,7 +326,7 @@ gd_status ens_enqueue(Ens &E, int n_steps, bool device_step) {
     }
     if (E.n_groups) {
       if (E.profile) GD_TRY(mark(E, 1));
-      GD_CUDA(launch_exchange(E.d_items, E.d_groups, E.n_groups, E.e_old, E.idx_tmp, E.spe, s0,
+      GD_CUDA(launch_exchange(E.d_items, E.d_groups, E.n_groups, E.spe, s0,
                               device_step ? E.d_step : nullptr, s));
       if (E.profile) GD_TRY(mark(E, 1));
       E.ctx->launches += 1;

@@ -63,13 +63,18 @@ struct KItem {
   int n_rep, n_tmp, n_lig_conf, n_prt;
   int steps_per_dump;    // exchange parity restarts every dump (<= 0: never)
   int rec_steps;
-  int pad1;
+  int step0;             // first MC step of the launch when KRun.item_step
   float move_scale[6];
   uint64_t seed;
   uint32_t stream_id, flags;
   const float *minus_beta;  // [n_tmp]
   int *acs_exchg;           // [n_tmp] by slot
   gd_record *record;        // [n_rep][rec_steps] or nullptr
+  // replica state of this item, indexed by its local replica number
+  float *m_old;             // [n_rep][6]
+  float *e_old;             // [n_rep][GD_NTERM]
+  int *idx_tmp;             // [n_rep]
+  int *acs_mc;              // [n_rep]
 };
 
 // Launch descriptor of one dock_kernel launch (by value).
@@ -93,13 +98,12 @@ struct KRun {
   const float *poses;    // [n_pose][6]
   float *terms;          // [n_pose][GD_NTERM]
   double *raw;           // [n_pose][GD_NRAW] or nullptr
-  // REMC: the first MC step is *step_ptr when step_ptr is set (graph replay)
+  // REMC: the first MC step is KItem.step0 with item_step (complexes at
+  // different steps in one launch), else *step_ptr when step_ptr is set
+  // (graph replay), else step0
   int step0, n_steps;
   const int *step_ptr;
-  float *m_old;          // [n_rep_total][6]
-  float *e_old;          // [n_rep_total][GD_NTERM]
-  int *idx_tmp;          // [n_rep_total]
-  int *acs_mc;           // [n_rep_total]
+  int item_step;
   int *err;              // error word (bounded waits)
 };
 
@@ -112,9 +116,8 @@ size_t dock_smem_bytes(int A, int P, int NA, int n_stages);
 
 // Kernel launchers (gd_kernels.cu); return the launch status.
 cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s);
-cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups,
-                            const float *e_old, int *idx_tmp, int spe, int step0,
-                            const int *step_ptr, cudaStream_t s);
+cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups, int spe,
+                            int step0, const int *step_ptr, cudaStream_t s);
 cudaError_t launch_advance(int *step_ptr, int spe, cudaStream_t s);
 cudaError_t launch_metropolis(int n, const float *e_new, const float *e_old,
                               const float *mbeta, const int *rep, const int *step,

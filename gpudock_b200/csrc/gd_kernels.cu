@@ -113,6 +113,152 @@ __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R)
   R[8] = c2 * c3;
 }
 
+// Warp 0 after the step's partial sums: cross-warp reduction in a fixed
+// order, hydrophobic transform per atom, normalisation and total in the
+// reference's order, then the pose output, or the Metropolis decision (with
+// the trajectory record) and, at the end of an interval, the in-CTA
+// temperature exchange.  Kept out of line so its registers do not burden the
+// pair loop.
+template <int MODE>
+__device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneState &me,
+                                         double *s_red, const float *s_hpc, int W, int P,
+                                         int MAXA, int lane, int rep, bool active, int prt_conf,
+                                         int lig_conf, int step) {
+  const KTables &T = I.T;
+  const int lna = T.lna;
+  const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
+    double S[NRED];
+#pragma unroll
+    for (int i = 0; i < NRED; ++i) S[i] = 0.0;
+    for (int w = 0; w < W; ++w) {
+      const double *red = s_red + (size_t)w * NRED * 32;
+#pragma unroll
+      for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
+    }
+    // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149)
+    for (int a = 0; a < lna; ++a) {
+      float h = 0.f;
+      for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
+      const int lt = T.lig_t[a];
+      const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
+      S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
+    }
+    const double n = (double)lna;
+    double raw[GD_NRAW];
+    raw[0] = S[0] / n;
+    raw[1] = S[1] / n;
+    raw[2] = S[2] / n;
+    raw[3] = S[3] / n;
+    raw[4] = -(S[4] / n / (double)T.s2pi);
+    raw[5] = S[5] / n;
+    raw[6] = S[6] / (double)T.kde3 / n;
+    raw[7] = log(S[7] / (double)T.pos);
+    {
+      // distance to the pocket (calcenergy_d.cu:278-283); centre = c + m
+      const float cx = __fadd_rn(lcx, me.m_new[0]);
+      const float cy = __fadd_rn(lcy, me.m_new[1]);
+      const float cz = __fadd_rn(lcz, me.m_new[2]);
+      const float dx = __fsub_rn(cx, T.pocket[0]);
+      const float dy = __fsub_rn(cy, T.pocket[1]);
+      const float dz = __fsub_rn(cz, T.pocket[2]);
+      raw[8] = (double)__fsqrt_rn(
+          __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+    }
+    float e[GD_NTERM];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+      e[i] = __fadd_rn(__fmul_rn(T.a_para[i], (float)raw[i]), T.b_para[i]);
+    float tot = __fmul_rn(T.w[0], e[0]);
+#pragma unroll
+    for (int i = 1; i < 9; ++i) tot = __fadd_rn(tot, __fmul_rn(T.w[i], e[i]));
+    e[9] = tot;
+
+    if (MODE == KMODE_POSES) {
+      if (active) {
+#pragma unroll
+        for (int i = 0; i < GD_NTERM; ++i) R.terms[(size_t)rep * GD_NTERM + i] = e[i];
+        if (R.raw) {
+#pragma unroll
+          for (int i = 0; i < GD_NRAW; ++i) R.raw[(size_t)rep * GD_NRAW + i] = raw[i];
+        }
+      }
+    } else {
+      int acc;
+      if (MODE == KMODE_INIT) {
+        acc = 1;  // forced accept with beta = 0 (montecarlo_d.cu:236-239)
+      } else {
+        acc = metropolis(e[9], me.e_old[9], me.mbeta, u01(me.u_bits));
+        if (active && I.record && step < I.rec_steps) {
+          gd_record *rc = I.record + (size_t)rep * I.rec_steps + step;
+          rc->idx_rep = rep;
+          rc->idx_prt = prt_conf;
+          rc->idx_tmp = me.idx_tmp;
+          rc->idx_lig = lig_conf;
+#pragma unroll
+          for (int i = 0; i < GD_NTERM; ++i) rc->e[i] = me.e_old[i];
+          rc->cmcc = 0.f;
+#pragma unroll
+          for (int i = 0; i < 6; ++i) rc->movematrix[i] = me.m_old[i];
+          rc->step = step;
+          rc->e_prop_total = e[9];
+          rc->accepted = acc;
+        }
+      }
+      if (acc) {
+        me.acs += 1;
+#pragma unroll
+        for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = e[i];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) me.m_old[i] = me.m_new[i];
+      }
+      // temperature exchange of the CTA's own groups at the end of every
+      // interval (exchangereplicas_d.cu:26-79); slot t of group gi is lane
+      // gi * n_tmp + t, so the groups never leave the CTA
+      if (MODE == KMODE_REMC && R.fused_exchange && ((step + 1) % R.spe) == 0 &&
+          (I.flags & GD_MC_EXCHANGE)) {
+        const int nt = I.n_tmp;
+        int *s_tmp = reinterpret_cast<int *>(s_red);          // 32 ints
+        float *s_en = reinterpret_cast<float *>(s_red) + 32;  // 32 floats
+        s_tmp[lane] = me.idx_tmp;
+        s_en[lane] = me.e_old[GD_E_TOTAL];
+        __syncwarp();
+        const int s0 = step + 1 - R.spe;
+        const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
+        const int mode_t = (within / R.spe) % 2;
+        if (active && (lane % nt) == 0) {
+          const int b = lane;  // first slot of this group
+          const uint32_t gid = (uint32_t)(prt_conf * I.n_lig_conf + (rep % I.n_lig_conf));
+          uint32_t k0, k1;
+          rng_key(I.seed, I.stream_id, k0, k1);
+          int orders[MAX_TMP];
+          for (int t = 0; t < nt; ++t) orders[s_tmp[b + t]] = t;
+          const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
+          for (int pair = 0; pair < maxpair; ++pair) {
+            const int i1 = (pair << 1) + mode_t;
+            const int o1 = orders[i1], o2 = orders[i1 + 1];
+            const int tt = s_tmp[b + o1];
+            const float mb1 = I.minus_beta[s_tmp[b + o1]];
+            const float mb2 = I.minus_beta[s_tmp[b + o2]];
+            const float delta =
+                __fmul_rn(__fsub_rn(mb1, mb2), __fsub_rn(s_en[b + o2], s_en[b + o1]));
+            const float prob = decision_expf(delta);
+            const U4 o =
+                philox4x32_10(U4{gid, (uint32_t)(s0 / R.spe), 2u, (uint32_t)pair}, k0, k1);
+            if (prob > u01(o.x)) {
+              s_tmp[b + o1] = s_tmp[b + o2];
+              s_tmp[b + o2] = tt;
+              atomicAdd(&I.acs_exchg[o1], 1);
+              atomicAdd(&I.acs_exchg[o2], 1);
+            }
+          }
+        }
+        __syncwarp();
+        me.idx_tmp = s_tmp[lane];
+        me.mbeta = I.minus_beta[me.idx_tmp];
+      }
+    }
+  }
+
 template <int MODE, int NA>
 __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     dock_kernel(const __grid_constant__ KRun R) {
@@ -183,7 +329,9 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   const bool resident = R.resident != 0;
   const int n_steps = (MODE == KMODE_REMC) ? R.n_steps : 1;
   const int passes = resident ? 1 : n_steps;
-  const int step_base = (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr : R.step0;
+  const int step_base = (MODE == KMODE_REMC && R.item_step)  ? I.step0
+                        : (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr
+                                                             : R.step0;
 
   // ---- producer warp: stages the protein conformation -------------------
   if (warp == W) {
@@ -213,7 +361,6 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   const int lna = T.lna;
   const bool active = lane < n_act;
   const int rep = lane_rep;                    // local replica / pose index
-  const int grep = I.rep_base + rep;           // replica in the state arrays
   const int lig_conf = (MODE == KMODE_POSES) ? R.lig_conf : rep % I.n_lig_conf;
   const float4 *orig = T.lig + (size_t)lig_conf * lna;
   LaneState &me = s_lane[lane];
@@ -222,7 +369,7 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   // this warp's atoms; padding atoms use the all-zero table row, no charge,
   // and sit far from everything
   int lto[NA];
-  float lq[NA], ox[NA], oy[NA], oz[NA];
+  float lq[NA];  // charge / el1: far-field electrostatics is q ele / (el1 d)
   int n_my = 0;
 #pragma unroll
   for (int k = 0; k < NA; ++k) {
@@ -231,14 +378,9 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       n_my = k + 1;
       lto[k] = T.lig_t[a] * GD_NPT;
       lq[k] = T.lig_q[a];
-      const float4 o = orig[a];
-      ox[k] = o.x;
-      oy[k] = o.y;
-      oz[k] = o.z;
     } else {
       lto[k] = GD_NLT * GD_NPT;
       lq[k] = 0.f;
-      ox[k] = oy[k] = oz[k] = FAR;
     }
   }
 
@@ -247,12 +389,12 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     me.idx_tmp = 0;
     me.mbeta = 0.f;
     if (MODE == KMODE_REMC) {
-      me.idx_tmp = R.idx_tmp[grep];
+      me.idx_tmp = I.idx_tmp[rep];
       me.mbeta = I.minus_beta[me.idx_tmp];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) me.m_old[i] = R.m_old[(size_t)grep * 6 + i];
+      for (int i = 0; i < 6; ++i) me.m_old[i] = I.m_old[(size_t)rep * 6 + i];
 #pragma unroll
-      for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = R.e_old[(size_t)grep * GD_NTERM + i];
+      for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = I.e_old[(size_t)rep * GD_NTERM + i];
     } else {
 #pragma unroll
       for (int i = 0; i < 6; ++i) me.m_old[i] = 0.f;
@@ -310,14 +452,20 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per atom
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
-      lx[k] = q00 * ox[k] + q01 * oy[k] + q02 * oz[k] + t0 + lcx;
-      ly[k] = q10 * ox[k] + q11 * oy[k] + q12 * oz[k] + t1 + lcy;
-      lz[k] = q20 * ox[k] + q21 * oy[k] + q22 * oz[k] + t2 + lcz;
+      // padding atoms sit far from everything
+      const float4 o = (k < n_my) ? orig[ag + A * k] : make_float4(FAR, FAR, FAR, 0.f);
+      lx[k] = q00 * o.x + q01 * o.y + q02 * o.z + t0 + lcx;
+      ly[k] = q10 * o.x + q11 * o.y + q12 * o.z + t1 + lcy;
+      lz[k] = q20 * o.x + q21 * o.y + q22 * o.z + t2 + lcz;
       if (k < n_my) my_hpc[(size_t)A * k * 32] = 0.f;
     }
 
     // ---- pair terms over the protein tiles -----------------------------------
-    double dvdw = 0.0, dele = 0.0, dpmf = 0.0, dpsp = 0.0, dhdb = 0.0;
+    // FP64 sums of this lane live in the warp's own reduction slots (read by
+    // warp 0 after the barrier), which keeps registers for the pair loop
+    double *my_red = s_red + (size_t)warp * NRED * 32 + lane;
+#pragma unroll
+    for (int i = 0; i < NRED; ++i) my_red[i * 32] = 0.0;
     const int t_first = resident ? pg : 0;
     const int t_step = resident ? P : 1;
     for (int t = t_first; t < n_tiles; t += t_step, ++it) {
@@ -330,56 +478,63 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
       for (int j0 = 0; j0 < nvalid; j0 += CHUNK) {
         const int j1 = min(nvalid, j0 + CHUNK);
-        float fvdw = 0.f, fele = 0.f, fpmf = 0.f, fpsp = 0.f, fhdb = 0.f;
+        float fvdw = 0.f, fnear = 0.f, fpmf = 0.f, fpsp = 0.f, fhdb = 0.f;
+        float fek[NA];  // sum of ele_p / d per atom (far-field electrostatics)
+#pragma unroll
+        for (int k = 0; k < NA; ++k) fek[k] = 0.f;
         for (int j = j0; j < j1; ++j) {
           const float4 Ap = ta[j];
           const float2 Bp = tb[j];
           const uint32_t meta = __float_as_uint(Bp.y);
           const int pt = (int)(meta & META_TYPE_MASK);
-          float d2v[NA], rv[NA];
           float mn = 3.0e38f;
-          // fast path: soft LJ, far-field electrostatics, contact PMF
+          // fast path: soft LJ, far-field electrostatics, contact PMF.  The LJ
+          // and PMF quotients share one reciprocal: with D1 = p4 and
+          // D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2); d2 >= 1e-6 keeps
+          // D1 D2 below 1e35.
 #pragma unroll
           for (int k = 0; k < NA; ++k) {
             const float4 Pk = s_tab_a[lto[k] + pt];  // p1a p2a pmf0 pmf1
             const float dx = lx[k] - Ap.x;
             const float dy = ly[k] - Ap.y;
             const float dz = lz[k] - Ap.z;
-            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float d2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1.0e-6f);
             const float r = frsqrt(d2);
             const float d = d2 * r;
             const float r2 = r * r;
-            const float r6 = r2 * r2 * r2;
-            const float r9 = r6 * r2 * r;
+            const float r3 = r2 * r;
+            const float r6 = r3 * r3;
+            const float r9 = r6 * r3;
             const float p1 = Pk.x * r9;
             const float p2 = Pk.y * r6;
             const float p4 = fmaf(p1, fmaf(lj0lj1, d2, lj0), 1.0f);
-            fvdw = fmaf(p1 - p2, frcp(p4), fvdw);
-            fele = fmaf(lq[k] * Ap.w, r * inv_el1, fele);
             const float dm = d - Pk.z;
-            const float ex = fex2(fmaf(-0.5f * LOG2E, d, 6.0f * LOG2E) * dm);
-            fpmf = fmaf(Pk.w, frcp(1.0f + ex), fpmf);
-            d2v[k] = d2;
-            rv[k] = r;
+            const float e1 = 1.0f + fex2(fmaf(-0.5f * LOG2E, d, 6.0f * LOG2E) * dm);
+            const float inv = frcp(p4 * e1);
+            fvdw = fmaf((p1 - p2) * e1, inv, fvdw);
+            fpmf = fmaf(Pk.w * p4, inv, fpmf);
+            fek[k] = fmaf(Ap.w, r, fek[k]);
             mn = fminf(mn, d2);
-          }
-          // hydrogen bond, for the type pairs that define one
-#pragma unroll
-          for (int k = 0; k < NA; ++k) {
+            // hydrogen bond, for the type pairs that define one
             const float2 Hk = s_tab_b[lto[k] + pt];  // hdb0 hdb1
             if (Hk.x > 0.1f) {
-              const float h3 = (d2v[k] * rv[k] - Hk.x) * Hk.y;
+              const float h3 = (d - Hk.x) * Hk.y;
               fhdb = fmaf(Hk.y, fex2((-0.5f * LOG2E) * h3 * h3), fhdb);
             }
           }
           // close-range terms, only when some lane has an atom within near_d2
+          // (distances recomputed: this path is taken for a few % of points)
           if (__any_sync(0xffffffffu, mn <= near_d2)) {
             const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
             const bool hflag = (meta & META_HPC_BIT) != 0u;
 #pragma unroll
             for (int k = 0; k < NA; ++k) {
-              const float d2 = d2v[k];
-              const float d = d2 * rv[k];
+              const float dx = lx[k] - Ap.x;
+              const float dy = ly[k] - Ap.y;
+              const float dz = lz[k] - Ap.z;
+              const float d2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1.0e-6f);
+              const float rk = frsqrt(d2);
+              const float d = d2 * rk;
               if (hflag && d2 <= 81.0f && k < n_my) {
                 float *h = my_hpc + (size_t)A * k * 32;
                 *h = fmaf(Bp.x, hpc_poly(d2), *h);
@@ -387,7 +542,7 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
               const float s1 = T.el1 * d;
               if (s1 < 1.0f) {
                 const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
-                fele = fmaf(lq[k] * Ap.w, gnear - rv[k] * inv_el1, fele);
+                fnear = fmaf(lq[k] * Ap.w, gnear - rk * inv_el1, fnear);
               }
               if (is_c2 && k < n_my) {
                 const float dm = d - s_tab_a[lto[k] + pt].z;
@@ -398,11 +553,14 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
             }
           }
         }
-        dvdw += (double)fvdw;
-        dele += (double)fele;
-        dpmf += (double)fpmf;
-        dpsp += (double)fpsp;
-        dhdb += (double)fhdb;
+        float fele = 0.f;
+#pragma unroll
+        for (int k = 0; k < NA; ++k) fele = fmaf(lq[k], fek[k], fele);
+        my_red[0 * 32] += (double)fvdw;
+        my_red[1 * 32] += (double)fele * (double)inv_el1 + (double)fnear;
+        my_red[2 * 32] += (double)fpmf;
+        my_red[3 * 32] += (double)fpsp;
+        my_red[4 * 32] += (double)fhdb;
       }
       if (!resident) {
         __syncwarp();
@@ -450,149 +608,13 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
 
     // ---- cross-warp reduction and finalisation (warp 0) ----------------------
     {
-      double *red = s_red + (size_t)warp * NRED * 32;
-      red[0 * 32 + lane] = dvdw;
-      red[1 * 32 + lane] = dele;
-      red[2 * 32 + lane] = dpmf;
-      red[3 * 32 + lane] = dpsp;
-      red[4 * 32 + lane] = dhdb;
-      red[5 * 32 + lane] = 0.0;
-      red[6 * 32 + lane] = dkde;
-      red[7 * 32 + lane] = dlhm;
+      my_red[6 * 32] = dkde;
+      my_red[7 * 32] = dlhm;
     }
     named_sync(1, W * 32);
-    if (warp == 0) {
-      double S[NRED];
-#pragma unroll
-      for (int i = 0; i < NRED; ++i) S[i] = 0.0;
-      for (int w = 0; w < W; ++w) {
-        const double *red = s_red + (size_t)w * NRED * 32;
-#pragma unroll
-        for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
-      }
-      // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149)
-      for (int a = 0; a < lna; ++a) {
-        float h = 0.f;
-        for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
-        const int lt = T.lig_t[a];
-        const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
-        S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
-      }
-      const double n = (double)lna;
-      double raw[GD_NRAW];
-      raw[0] = S[0] / n;
-      raw[1] = S[1] / n;
-      raw[2] = S[2] / n;
-      raw[3] = S[3] / n;
-      raw[4] = -(S[4] / n / (double)T.s2pi);
-      raw[5] = S[5] / n;
-      raw[6] = S[6] / (double)T.kde3 / n;
-      raw[7] = log(S[7] / (double)T.pos);
-      {
-        // distance to the pocket (calcenergy_d.cu:278-283); centre = c + m
-        const float cx = __fadd_rn(lcx, me.m_new[0]);
-        const float cy = __fadd_rn(lcy, me.m_new[1]);
-        const float cz = __fadd_rn(lcz, me.m_new[2]);
-        const float dx = __fsub_rn(cx, T.pocket[0]);
-        const float dy = __fsub_rn(cy, T.pocket[1]);
-        const float dz = __fsub_rn(cz, T.pocket[2]);
-        raw[8] = (double)__fsqrt_rn(
-            __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
-      }
-      float e[GD_NTERM];
-#pragma unroll
-      for (int i = 0; i < 9; ++i)
-        e[i] = __fadd_rn(__fmul_rn(T.a_para[i], (float)raw[i]), T.b_para[i]);
-      float tot = __fmul_rn(T.w[0], e[0]);
-#pragma unroll
-      for (int i = 1; i < 9; ++i) tot = __fadd_rn(tot, __fmul_rn(T.w[i], e[i]));
-      e[9] = tot;
-
-      if (MODE == KMODE_POSES) {
-        if (active) {
-#pragma unroll
-          for (int i = 0; i < GD_NTERM; ++i) R.terms[(size_t)rep * GD_NTERM + i] = e[i];
-          if (R.raw) {
-#pragma unroll
-            for (int i = 0; i < GD_NRAW; ++i) R.raw[(size_t)rep * GD_NRAW + i] = raw[i];
-          }
-        }
-      } else {
-        int acc;
-        if (MODE == KMODE_INIT) {
-          acc = 1;  // forced accept with beta = 0 (montecarlo_d.cu:236-239)
-        } else {
-          acc = metropolis(e[9], me.e_old[9], me.mbeta, u01(me.u_bits));
-          if (active && I.record && step < I.rec_steps) {
-            gd_record *rc = I.record + (size_t)rep * I.rec_steps + step;
-            rc->idx_rep = rep;
-            rc->idx_prt = prt_conf;
-            rc->idx_tmp = me.idx_tmp;
-            rc->idx_lig = lig_conf;
-#pragma unroll
-            for (int i = 0; i < GD_NTERM; ++i) rc->e[i] = me.e_old[i];
-            rc->cmcc = 0.f;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) rc->movematrix[i] = me.m_old[i];
-            rc->step = step;
-            rc->e_prop_total = e[9];
-            rc->accepted = acc;
-          }
-        }
-        if (acc) {
-          me.acs += 1;
-#pragma unroll
-          for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = e[i];
-#pragma unroll
-          for (int i = 0; i < 6; ++i) me.m_old[i] = me.m_new[i];
-        }
-        // temperature exchange of the CTA's own groups at the end of every
-        // interval (exchangereplicas_d.cu:26-79); slot t of group gi is lane
-        // gi * n_tmp + t, so the groups never leave the CTA
-        if (MODE == KMODE_REMC && R.fused_exchange && ((step + 1) % R.spe) == 0 &&
-            (I.flags & GD_MC_EXCHANGE)) {
-          const int nt = I.n_tmp;
-          int *s_tmp = reinterpret_cast<int *>(s_red);          // 32 ints
-          float *s_en = reinterpret_cast<float *>(s_red) + 32;  // 32 floats
-          s_tmp[lane] = me.idx_tmp;
-          s_en[lane] = me.e_old[GD_E_TOTAL];
-          __syncwarp();
-          const int s0 = step + 1 - R.spe;
-          const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
-          const int mode_t = (within / R.spe) % 2;
-          if (active && (lane % nt) == 0) {
-            const int b = lane;  // first slot of this group
-            const uint32_t gid = (uint32_t)(prt_conf * I.n_lig_conf + (rep % I.n_lig_conf));
-            uint32_t k0, k1;
-            rng_key(I.seed, I.stream_id, k0, k1);
-            int orders[MAX_TMP];
-            for (int t = 0; t < nt; ++t) orders[s_tmp[b + t]] = t;
-            const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
-            for (int pair = 0; pair < maxpair; ++pair) {
-              const int i1 = (pair << 1) + mode_t;
-              const int o1 = orders[i1], o2 = orders[i1 + 1];
-              const int tt = s_tmp[b + o1];
-              const float mb1 = I.minus_beta[s_tmp[b + o1]];
-              const float mb2 = I.minus_beta[s_tmp[b + o2]];
-              const float delta =
-                  __fmul_rn(__fsub_rn(mb1, mb2), __fsub_rn(s_en[b + o2], s_en[b + o1]));
-              const float prob = decision_expf(delta);
-              const U4 o =
-                  philox4x32_10(U4{gid, (uint32_t)(s0 / R.spe), 2u, (uint32_t)pair}, k0, k1);
-              if (prob > u01(o.x)) {
-                s_tmp[b + o1] = s_tmp[b + o2];
-                s_tmp[b + o2] = tt;
-                atomicAdd(&I.acs_exchg[o1], 1);
-                atomicAdd(&I.acs_exchg[o2], 1);
-              }
-            }
-          }
-          __syncwarp();
-          me.idx_tmp = s_tmp[lane];
-          me.mbeta = I.minus_beta[me.idx_tmp];
-        }
-      }
-    }
+    if (warp == 0)
+      finish_step<MODE>(R, I, me, s_red, s_hpc, W, P, MAXA, lane, rep, active, prt_conf,
+                        lig_conf, step);
     // the next step's first barrier orders warp 0's updates (and its use of
     // s_red for the exchange) before any other warp touches them again
   }
@@ -600,15 +622,15 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   // ---- write the replica state back ----------------------------------------
   if (MODE != KMODE_POSES && warp == 0 && active) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i) R.m_old[(size_t)grep * 6 + i] = me.m_old[i];
+    for (int i = 0; i < 6; ++i) I.m_old[(size_t)rep * 6 + i] = me.m_old[i];
 #pragma unroll
-    for (int i = 0; i < GD_NTERM; ++i) R.e_old[(size_t)grep * GD_NTERM + i] = me.e_old[i];
+    for (int i = 0; i < GD_NTERM; ++i) I.e_old[(size_t)rep * GD_NTERM + i] = me.e_old[i];
     if (MODE == KMODE_INIT) {
-      R.acs_mc[grep] = 0;
-      R.idx_tmp[grep] = (rep / I.n_lig_conf) % I.n_tmp;
+      I.acs_mc[rep] = 0;
+      I.idx_tmp[rep] = (rep / I.n_lig_conf) % I.n_tmp;
     } else {
-      R.acs_mc[grep] += me.acs;
-      if (R.fused_exchange) R.idx_tmp[grep] = me.idx_tmp;
+      I.acs_mc[rep] += me.acs;
+      if (R.fused_exchange) I.idx_tmp[rep] = me.idx_tmp;
     }
   }
 }
@@ -617,14 +639,15 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
 // group (exchangereplicas_d.cu:26-79).  Pairs of adjacent temperature
 // indices (2 pair + mode_t, 2 pair + mode_t + 1) swap their slots when
 // exp((mb1 - mb2)(E2 - E1)) > u; the counters are kept per slot.
-__global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_groups,
-                                const float *e_old, int *idx_tmp_g, int spe, int step0,
-                                const int *step_ptr) {
+__global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_groups, int spe,
+                                int step0, const int *step_ptr) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_groups) return;
   const KGroup G = groups[g];
   const KItem &I = items[G.item];
-  const int s0 = step_ptr ? *step_ptr : step0;
+  // interval start: the device counter, the launch's step, or (step0 < 0)
+  // each item's own step
+  const int s0 = step_ptr ? *step_ptr : (step0 >= 0 ? step0 : I.step0);
   const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
   const int mode_t = (within / spe) % 2;
   const int round = s0 / spe;
@@ -632,9 +655,9 @@ __global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_
   int temps[MAX_TMP], orders[MAX_TMP];
   float en[MAX_TMP];
   for (int t = 0; t < nt; ++t) {
-    const int r = I.rep_base + nt * nl * G.p + nl * t + G.l;
-    temps[t] = idx_tmp_g[r];
-    en[t] = e_old[(size_t)r * GD_NTERM + GD_E_TOTAL];
+    const int r = nt * nl * G.p + nl * t + G.l;
+    temps[t] = I.idx_tmp[r];
+    en[t] = I.e_old[(size_t)r * GD_NTERM + GD_E_TOTAL];
   }
   for (int t = 0; t < nt; ++t) orders[temps[t]] = t;
   uint32_t k0, k1;
@@ -658,7 +681,7 @@ __global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_
       atomicAdd(&I.acs_exchg[o2], 1);
     }
   }
-  for (int t = 0; t < nt; ++t) idx_tmp_g[I.rep_base + nt * nl * G.p + nl * t + G.l] = temps[t];
+  for (int t = 0; t < nt; ++t) I.idx_tmp[nt * nl * G.p + nl * t + G.l] = temps[t];
 }
 
 __global__ void advance_kernel(int *step_ptr, int spe) {
@@ -750,12 +773,11 @@ cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s) {
   }
 }
 
-cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups,
-                            const float *e_old, int *idx_tmp, int spe, int step0,
-                            const int *step_ptr, cudaStream_t s) {
+cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups, int spe,
+                            int step0, const int *step_ptr, cudaStream_t s) {
   if (n_groups <= 0) return cudaSuccess;
-  exchange_kernel<<<(n_groups + 127) / 128, 128, 0, s>>>(items, groups, n_groups, e_old,
-                                                          idx_tmp, spe, step0, step_ptr);
+  exchange_kernel<<<(n_groups + 127) / 128, 128, 0, s>>>(items, groups, n_groups, spe, step0,
+                                                          step_ptr);
   return cudaGetLastError();
 }
 

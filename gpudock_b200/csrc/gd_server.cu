@@ -1,0 +1,673 @@
+// gd_server.cu -- the serving form: a request loop with continuous batching.
+//
+// Docking requests (a ligand ensemble + pocket template against one of the
+// server's resident proteins, with its own MC parameters) are queued by
+// gd_server_submit and admitted by a scheduler thread while the HBM budget
+// and the slot count allow.  Every scheduler iteration advances all admitted
+// requests by `steps_per_launch` MC steps in one launch per launch shape:
+// each request keeps its own step counter (KItem.step0), replica state and
+// random stream, so requests that arrived at different times share launches
+// and a request's results do not depend on what else is running.  Finished
+// requests are copied out and their memory returns to the budget before the
+// next iteration admits more.
+//
+// There is no counterpart in the reference (Run() handles one complex per
+// process, run.cu:41-353); the semantics of every request are those of Run.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gd_common.h"
+
+using namespace gd;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+enum ReqState { RQ_QUEUED, RQ_ACTIVE, RQ_DONE, RQ_CANCELLED, RQ_FAILED };
+
+// A protein resident for the server's lifetime (device tables + host copy of
+// the point properties for validating requests).
+struct SrvProtein {
+  gd_dcomplex *dcx = nullptr;
+  std::vector<float> x, y, z, ele, hpp;
+  std::vector<int> t, c, seq3r, hflag;
+  gd_protein prt{};
+  size_t bytes = 0;
+};
+
+struct Req {
+  uint64_t id = 0;
+  int protein = 0;
+  ReqState state = RQ_QUEUED;
+  gd_status err = GD_OK;
+  bool cancel = false;
+  // owned host copy of the request
+  std::vector<float> lx, ly, lz, lc, psp, kx, ky, kz, mx, my, mz, tcc, mb;
+  std::vector<int> lt, ln, kt;
+  gd_enepara ff{};
+  gd_complex cx{};
+  gd_mc_params mc{};
+  int n_rep = 0;
+  size_t bytes = 0;
+  Clock::time_point t_submit, t_start, t_done;
+  // device side while active
+  gd_dcomplex *dcx = nullptr;
+  float *d_m_old = nullptr, *d_e_old = nullptr, *d_mb = nullptr;
+  int *d_idx = nullptr, *d_acs = nullptr, *d_acx = nullptr;
+  int step = 0;
+  KItem item{};
+  // results
+  std::vector<float> energy, movematrix;
+  std::vector<int> acs, idx, acx;
+};
+
+}  // namespace
+
+struct gd_server {
+  gd_ctx *ctx = nullptr;
+  size_t budget = 0;
+  int max_active = 0;
+  int steps_per_launch = 0;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;       // scheduler wake-up
+  std::condition_variable done_cv;  // request completion
+  bool stop = false;
+  std::vector<std::unique_ptr<SrvProtein>> proteins;
+  size_t protein_bytes = 0;
+  std::deque<Req *> queue;
+  std::vector<Req *> active;
+  std::unordered_map<uint64_t, std::unique_ptr<Req>> reqs;
+  uint64_t next_id = 1;
+  size_t bytes_in_use = 0;
+  // statistics
+  uint64_t n_done = 0, n_iter = 0, n_launch = 0;
+  double busy_s = 0.0;
+  // device staging for the launch descriptors, grown on demand
+  KItem *d_items = nullptr;
+  int *d_cta = nullptr;  // [3][cap_cta]
+  KGroup *d_groups = nullptr;
+  size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
+  cudaEvent_t ev = nullptr;
+};
+
+namespace {
+
+// Device bytes a request holds while active (tables + replica state).
+size_t request_bytes(const gd_complex *cx, int n_rep) {
+  size_t b = (size_t)TAB_ROWS * GD_NPT * 24;
+  b += (size_t)cx->lig.n_conf * cx->lig.lna * 16 + (size_t)cx->lig.lna * 8;
+  b += (size_t)GD_NLT * cx->psp.n_col * 4;
+  b += (size_t)cx->kde.pnk * 16 + (GD_NLT + 1) * 4;
+  b += (size_t)cx->mcs.pos * cx->lig.lna * 16 + (size_t)cx->mcs.pos * 8;
+  b += (size_t)n_rep * (6 + GD_NTERM + 2) * 4 + 3 * MAX_TMP * 4;
+  return b;
+}
+
+template <typename T>
+std::vector<T> vcopy(const T *p, size_t n) {
+  return p ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+void release_device(gd_server *S, Req *r) {
+  cudaStream_t s = S->ctx->stream;
+  if (r->d_m_old) cudaFreeAsync(r->d_m_old, s);
+  if (r->d_e_old) cudaFreeAsync(r->d_e_old, s);
+  if (r->d_mb) cudaFreeAsync(r->d_mb, s);
+  if (r->d_idx) cudaFreeAsync(r->d_idx, s);
+  if (r->d_acs) cudaFreeAsync(r->d_acs, s);
+  if (r->d_acx) cudaFreeAsync(r->d_acx, s);
+  r->d_m_old = r->d_e_old = r->d_mb = nullptr;
+  r->d_idx = r->d_acs = r->d_acx = nullptr;
+  if (r->dcx) {
+    cudaStreamSynchronize(s);
+    dcx_release(r->dcx);
+    r->dcx = nullptr;
+  }
+}
+
+template <typename T>
+gd_status grow(T **p, size_t *cap, size_t need) {
+  if (need <= *cap) return GD_OK;
+  size_t n = std::max<size_t>(need, *cap * 2 + 64);
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  GD_CUDA(cudaMalloc(p, n * sizeof(T)));
+  *cap = n;
+  return GD_OK;
+}
+
+// Uploads the request's tables, allocates its state and fills its KItem.
+gd_status admit(gd_server *S, Req *r) {
+  SrvProtein &P = *S->proteins[r->protein];
+  GD_TRY(gd_complex_upload_shared(S->ctx, &r->cx, P.dcx, 0, P.prt.n_conf, &r->dcx));
+  cudaStream_t s = S->ctx->stream;
+  const size_t n = (size_t)r->n_rep;
+  GD_CUDA(cudaMallocAsync(&r->d_m_old, n * 6 * sizeof(float), s));
+  GD_CUDA(cudaMallocAsync(&r->d_e_old, n * GD_NTERM * sizeof(float), s));
+  GD_CUDA(cudaMallocAsync(&r->d_mb, MAX_TMP * sizeof(float), s));
+  GD_CUDA(cudaMallocAsync(&r->d_idx, n * sizeof(int), s));
+  GD_CUDA(cudaMallocAsync(&r->d_acs, n * sizeof(int), s));
+  GD_CUDA(cudaMallocAsync(&r->d_acx, MAX_TMP * sizeof(int), s));
+  GD_CUDA(cudaMemsetAsync(r->d_acx, 0, MAX_TMP * sizeof(int), s));
+  GD_CUDA(cudaMemcpyAsync(r->d_mb, r->mb.data(), r->mb.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, s));
+  KItem &I = r->item;
+  std::memset(&I, 0, sizeof(I));
+  I.T = r->dcx->T;
+  I.rep_base = 0;
+  I.n_tmp = r->mc.n_tmp;
+  I.n_lig_conf = I.T.n_lig;
+  I.n_prt = I.T.n_prt;
+  I.n_rep = r->n_rep;
+  I.steps_per_dump = r->mc.steps_per_dump;
+  for (int k = 0; k < 6; ++k) I.move_scale[k] = r->mc.move_scale[k];
+  I.seed = r->mc.seed;
+  I.stream_id = r->mc.stream_id;
+  I.flags = r->mc.flags & ~GD_MC_RECORD;
+  I.minus_beta = r->d_mb;
+  I.acs_exchg = r->d_acx;
+  I.record = nullptr;
+  I.m_old = r->d_m_old;
+  I.e_old = r->d_e_old;
+  I.idx_tmp = r->d_idx;
+  I.acs_mc = r->d_acs;
+  r->step = 0;
+  return GD_OK;
+}
+
+struct ShapePlan {
+  Tile tile;
+  int ns = 0, res = 0, gm = 0, spe = 0;
+  std::vector<std::tuple<double, int, int, int>> ctas;  // cost, item, rep0/group, n
+};
+
+// One launch per launch shape over the given requests (KRun item_step).
+gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n_steps) {
+  if (rs.empty()) return GD_OK;
+  cudaStream_t s = S->ctx->stream;
+  std::vector<KItem> items;
+  items.reserve(rs.size());
+  using Key = std::tuple<int, int, int, int, int, int, int>;
+  std::map<Key, ShapePlan> plans;
+  std::vector<KGroup> groups;
+  for (size_t i = 0; i < rs.size(); ++i) {
+    Req *r = rs[i];
+    r->item.step0 = r->step;
+    items.push_back(r->item);
+    const KItem &I = r->item;
+    Tile t = tile_for(S->ctx, I.T);
+    int ns, res;
+    pick_stages(I.T, t, &ns, &res);
+    if (!res) t.P = 1;
+    const int nt = I.n_tmp, nl = I.n_lig_conf;
+    const bool gm = (32 % nt) == 0;
+    const int spe = r->mc.steps_per_exchange;
+    ShapePlan &pl = plans[Key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe}];
+    pl.tile = t;
+    pl.ns = ns;
+    pl.res = res;
+    pl.gm = gm ? 1 : 0;
+    pl.spe = spe;
+    const double cost = (double)I.T.lna * I.T.pnp;
+    if (gm) {
+      const int G = 32 / nt;
+      for (int p = 0; p < I.n_prt; ++p)
+        for (int l0 = 0; l0 < nl; l0 += G)
+          pl.ctas.emplace_back(cost, (int)i, p * nl + l0, std::min(G, nl - l0) * nt);
+    } else {
+      const int per_p = nt * nl;
+      for (int p = 0; p < I.n_prt; ++p)
+        for (int j = 0; j < per_p; j += 32)
+          pl.ctas.emplace_back(cost, (int)i, p * per_p + j, std::min(32, per_p - j));
+      if (mode == KMODE_REMC && (I.flags & GD_MC_EXCHANGE))
+        for (int p = 0; p < I.n_prt; ++p)
+          for (int l = 0; l < nl; ++l) groups.push_back(KGroup{(int)i, p, l, 0});
+    }
+  }
+  size_t n_cta = 0;
+  for (auto &kv : plans) n_cta += kv.second.ctas.size();
+  GD_TRY(grow(&S->d_items, &S->cap_items, items.size()));
+  GD_TRY(grow(&S->d_cta, &S->cap_cta, 3 * n_cta));
+  GD_TRY(grow(&S->d_groups, &S->cap_groups, std::max<size_t>(groups.size(), 1)));
+  // the descriptors of the previous launch may still be read: order the
+  // copies after it on the same stream (pageable copies stage synchronously)
+  GD_CUDA(cudaMemcpyAsync(S->d_items, items.data(), items.size() * sizeof(KItem),
+                          cudaMemcpyHostToDevice, s));
+  std::vector<int> cta(3 * n_cta);
+  size_t off = 0;
+  std::vector<std::pair<const ShapePlan *, size_t>> launches;
+  for (auto &kv : plans) {
+    ShapePlan &pl = kv.second;
+    std::stable_sort(pl.ctas.begin(), pl.ctas.end(),
+                     [](const auto &a, const auto &b) { return std::get<0>(a) > std::get<0>(b); });
+    launches.emplace_back(&pl, off);
+    for (size_t c = 0; c < pl.ctas.size(); ++c) {
+      cta[off + c] = std::get<1>(pl.ctas[c]);
+      cta[n_cta + off + c] = std::get<2>(pl.ctas[c]);
+      cta[2 * n_cta + off + c] = std::get<3>(pl.ctas[c]);
+    }
+    off += pl.ctas.size();
+  }
+  GD_CUDA(cudaMemcpyAsync(S->d_cta, cta.data(), cta.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          s));
+  if (!groups.empty())
+    GD_CUDA(cudaMemcpyAsync(S->d_groups, groups.data(), groups.size() * sizeof(KGroup),
+                            cudaMemcpyHostToDevice, s));
+  for (auto &lp : launches) {
+    const ShapePlan &pl = *lp.first;
+    KRun R{};
+    R.mode = mode;
+    R.A = pl.tile.A;
+    R.P = pl.tile.P;
+    R.n_stages = pl.ns;
+    R.resident = pl.res;
+    R.items = S->d_items;
+    R.cta_item = S->d_cta + lp.second;
+    R.cta_rep0 = S->d_cta + n_cta + lp.second;
+    R.cta_nrep = S->d_cta + 2 * n_cta + lp.second;
+    R.group_major = pl.gm;
+    R.fused_exchange = pl.gm;
+    R.spe = pl.spe;  // every request of a launch shares its exchange interval
+    R.step0 = 0;
+    R.n_steps = n_steps;
+    R.item_step = 1;
+    R.err = S->ctx->d_err;
+    GD_CUDA(launch_dock(R, pl.tile.NA, (int)pl.ctas.size(), s));
+    S->ctx->launches += 1;
+    S->n_launch += 1;
+  }
+  if (!groups.empty()) {
+    GD_CUDA(launch_exchange(S->d_items, S->d_groups, (int)groups.size(), S->steps_per_launch, -1,
+                            nullptr, s));
+    S->ctx->launches += 1;
+    S->n_launch += 1;
+  }
+  return GD_OK;
+}
+
+gd_status copy_out(gd_server *S, Req *r) {
+  cudaStream_t s = S->ctx->stream;
+  const size_t n = (size_t)r->n_rep;
+  r->energy.resize(n * GD_NTERM);
+  r->movematrix.resize(n * 6);
+  r->acs.resize(n);
+  r->idx.resize(n);
+  r->acx.resize(r->mc.n_tmp);
+  GD_CUDA(cudaMemcpyAsync(r->energy.data(), r->d_e_old, n * GD_NTERM * 4, cudaMemcpyDeviceToHost,
+                          s));
+  GD_CUDA(cudaMemcpyAsync(r->movematrix.data(), r->d_m_old, n * 24, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->acs.data(), r->d_acs, n * 4, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->idx.data(), r->d_idx, n * 4, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->acx.data(), r->d_acx, r->mc.n_tmp * 4, cudaMemcpyDeviceToHost, s));
+  return GD_OK;
+}
+
+void finish(gd_server *S, Req *r, ReqState st, gd_status err) {
+  release_device(S, r);
+  r->state = st;
+  r->err = err;
+  r->t_done = Clock::now();
+  S->bytes_in_use -= r->bytes;
+  if (st == RQ_DONE) S->n_done += 1;
+}
+
+void scheduler(gd_server *S) {
+  cudaSetDevice(S->ctx->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  while (!S->stop) {
+    // drop cancelled requests still in the queue
+    for (auto it = S->queue.begin(); it != S->queue.end();) {
+      if ((*it)->cancel) {
+        (*it)->state = RQ_CANCELLED;
+        (*it)->t_done = Clock::now();
+        it = S->queue.erase(it);
+        S->done_cv.notify_all();
+      } else {
+        ++it;
+      }
+    }
+    // admit while slots and HBM budget allow (first come, first served)
+    std::vector<Req *> fresh;
+    while (!S->queue.empty() &&
+           (S->max_active <= 0 || (int)(S->active.size() + fresh.size()) < S->max_active) &&
+           S->protein_bytes + S->bytes_in_use + S->queue.front()->bytes <= S->budget) {
+      Req *r = S->queue.front();
+      S->queue.pop_front();
+      S->bytes_in_use += r->bytes;
+      r->state = RQ_ACTIVE;
+      r->t_start = Clock::now();
+      fresh.push_back(r);
+    }
+    if (fresh.empty() && S->active.empty()) {
+      S->cv.wait_for(lk, std::chrono::milliseconds(50));
+      continue;
+    }
+    // cancelled active requests leave at the iteration boundary
+    for (auto it = S->active.begin(); it != S->active.end();) {
+      if ((*it)->cancel) {
+        finish(S, *it, RQ_CANCELLED, GD_ECANCELLED);
+        it = S->active.erase(it);
+        S->done_cv.notify_all();
+      } else {
+        ++it;
+      }
+    }
+    std::vector<Req *> todo = S->active;
+    lk.unlock();
+
+    const auto t0 = Clock::now();
+    std::vector<Req *> ok_fresh;
+    std::vector<std::pair<Req *, gd_status>> failed;
+    for (Req *r : fresh) {
+      gd_status st = admit(S, r);
+      if (st == GD_OK)
+        ok_fresh.push_back(r);
+      else
+        failed.emplace_back(r, st);
+    }
+    gd_status st = launch_all(S, ok_fresh, KMODE_INIT, 1);
+    for (Req *r : ok_fresh) todo.push_back(r);
+    if (st == GD_OK) st = launch_all(S, todo, KMODE_REMC, S->steps_per_launch);
+    if (st == GD_OK) {
+      cudaEventRecord(S->ev, S->ctx->stream);
+      cudaEventSynchronize(S->ev);
+      st = ctx_check(S->ctx);
+    }
+    std::vector<Req *> finished;
+    for (Req *r : todo) {
+      r->step += S->steps_per_launch;
+      if (st == GD_OK && r->step >= r->mc.steps_total) {
+        if (copy_out(S, r) == GD_OK) finished.push_back(r);
+      }
+    }
+    if (!finished.empty()) cudaStreamSynchronize(S->ctx->stream);
+
+    lk.lock();
+    S->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
+    S->n_iter += 1;
+    for (auto &f : failed) finish(S, f.first, RQ_FAILED, f.second);
+    S->active = todo;
+    if (st != GD_OK) {
+      for (Req *r : S->active) finish(S, r, RQ_FAILED, st);
+      S->active.clear();
+    } else {
+      for (Req *r : finished) {
+        finish(S, r, RQ_DONE, GD_OK);
+        S->active.erase(std::find(S->active.begin(), S->active.end(), r));
+      }
+    }
+    if (!failed.empty() || !finished.empty() || st != GD_OK) S->done_cv.notify_all();
+  }
+}
+
+gd_status copy_request(gd_server *S, int protein_id, const gd_complex *cx,
+                       const gd_mc_params *mc, Req *r) {
+  const SrvProtein &P = *S->proteins[protein_id];
+  const gd_ligand &L = cx->lig;
+  const size_t nl = (size_t)L.n_conf * L.lna;
+  r->lx = vcopy(L.x, nl);
+  r->ly = vcopy(L.y, nl);
+  r->lz = vcopy(L.z, nl);
+  r->lt = vcopy(L.t, (size_t)L.lna);
+  r->lc = vcopy(L.c, (size_t)L.lna);
+  r->ln = vcopy(L.n, (size_t)L.lna);
+  r->psp = vcopy(cx->psp.psp, (size_t)GD_NLT * cx->psp.n_col);
+  r->kx = vcopy(cx->kde.x, (size_t)cx->kde.pnk);
+  r->ky = vcopy(cx->kde.y, (size_t)cx->kde.pnk);
+  r->kz = vcopy(cx->kde.z, (size_t)cx->kde.pnk);
+  r->kt = vcopy(cx->kde.t, (size_t)cx->kde.pnk);
+  const size_t nm = (size_t)cx->mcs.pos * cx->mcs.n_field;
+  r->mx = vcopy(cx->mcs.x, nm);
+  r->my = vcopy(cx->mcs.y, nm);
+  r->mz = vcopy(cx->mcs.z, nm);
+  r->tcc = vcopy(cx->mcs.tcc, (size_t)cx->mcs.pos);
+  r->ff = *cx->ff;
+  r->mb = vcopy(mc->minus_beta, (size_t)mc->n_tmp);
+  r->cx = *cx;
+  r->cx.lig.x = r->lx.data();
+  r->cx.lig.y = r->ly.data();
+  r->cx.lig.z = r->lz.data();
+  r->cx.lig.t = r->lt.data();
+  r->cx.lig.c = r->lc.data();
+  r->cx.lig.n = r->ln.data();
+  r->cx.psp.psp = r->psp.data();
+  r->cx.kde.x = r->kx.data();
+  r->cx.kde.y = r->ky.data();
+  r->cx.kde.z = r->kz.data();
+  r->cx.kde.t = r->kt.data();
+  r->cx.mcs.x = r->mx.data();
+  r->cx.mcs.y = r->my.data();
+  r->cx.mcs.z = r->mz.data();
+  r->cx.mcs.tcc = r->tcc.data();
+  r->cx.ff = &r->ff;
+  r->cx.prt = P.prt;  // the resident protein
+  r->mc = *mc;
+  r->mc.minus_beta = r->mb.data();
+  r->protein = protein_id;
+  r->n_rep = P.prt.n_conf * L.n_conf * mc->n_tmp;
+  r->bytes = request_bytes(&r->cx, r->n_rep);
+  return GD_OK;
+}
+
+}  // namespace
+
+extern "C" gd_status gd_server_create(int device, size_t hbm_budget_bytes, int max_active,
+                                      int steps_per_launch, gd_server **out) {
+  if (!out) return fail(GD_EINVAL, "gd_server_create: out is NULL");
+  *out = nullptr;
+  if (steps_per_launch < 1) return fail(GD_EINVAL, "steps_per_launch=%d", steps_per_launch);
+  gd_ctx *ctx = nullptr;
+  GD_TRY(gd_ctx_create(device, nullptr, &ctx));
+  gd_server *S = new (std::nothrow) gd_server;
+  if (!S) {
+    ctx_release(ctx);
+    return fail(GD_ENOMEM, "host allocation");
+  }
+  S->ctx = ctx;
+  S->budget = hbm_budget_bytes;
+  S->max_active = max_active > 0 ? max_active : 2 * ctx->n_sm;
+  S->steps_per_launch = steps_per_launch;
+  cudaEventCreateWithFlags(&S->ev, cudaEventBlockingSync);
+  S->th = std::thread(scheduler, S);
+  *out = S;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_server_add_protein(gd_server *S, const gd_complex *cx, int *protein_id) {
+  if (!S || !cx || !protein_id) return fail(GD_EINVAL, "gd_server_add_protein: NULL argument");
+  GD_TRY(gd_complex_validate(cx));
+  auto P = std::make_unique<SrvProtein>();
+  const gd_protein &src = cx->prt;
+  const size_t np = (size_t)src.pnp, nc = (size_t)src.n_conf * src.pnp;
+  P->x = vcopy(src.x, nc);
+  P->y = vcopy(src.y, nc);
+  P->z = vcopy(src.z, nc);
+  P->t = vcopy(src.t, np);
+  P->c = vcopy(src.c, np);
+  P->ele = vcopy(src.ele, np);
+  P->seq3r = vcopy(src.seq3r, np);
+  P->hflag = vcopy(src.c0_and_d12_or_c2, np);
+  P->hpp = vcopy(src.hpp, np);
+  P->prt = src;
+  P->prt.x = P->x.data();
+  P->prt.y = P->y.data();
+  P->prt.z = P->z.data();
+  P->prt.t = P->t.data();
+  P->prt.c = P->c.data();
+  P->prt.ele = P->ele.data();
+  P->prt.seq3r = P->seq3r.data();
+  P->prt.c0_and_d12_or_c2 = P->hflag.data();
+  P->prt.hpp = P->hpp.data();
+  std::lock_guard<std::mutex> g(S->mu);
+  cudaSetDevice(S->ctx->device);
+  GD_TRY(gd_complex_upload(S->ctx, cx, &P->dcx));
+  P->bytes = gd_complex_device_bytes(P->dcx);
+  if (S->protein_bytes + P->bytes > S->budget) {
+    dcx_release(P->dcx);
+    return fail(GD_EBUDGET, "protein needs %zu bytes, budget %zu already holds %zu", P->bytes,
+                S->budget, S->protein_bytes);
+  }
+  S->protein_bytes += P->bytes;
+  *protein_id = (int)S->proteins.size();
+  S->proteins.push_back(std::move(P));
+  return GD_OK;
+}
+
+extern "C" gd_status gd_server_submit(gd_server *S, int protein_id, const gd_complex *cx,
+                                      const gd_mc_params *mc, uint64_t *req_id) {
+  if (!S || !cx || !mc || !req_id) return fail(GD_EINVAL, "gd_server_submit: NULL argument");
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    if (protein_id < 0 || protein_id >= (int)S->proteins.size())
+      return fail(GD_EINVAL, "unknown protein %d", protein_id);
+  }
+  if (mc->n_tmp < 1 || mc->n_tmp > MAX_TMP || !mc->minus_beta)
+    return fail(GD_EINVAL, "n_tmp=%d", mc->n_tmp);
+  if (mc->steps_per_exchange < 1 || S->steps_per_launch % mc->steps_per_exchange != 0)
+    return fail(GD_EINVAL, "steps_per_exchange %d does not divide the server's %d steps per "
+                "launch", mc->steps_per_exchange, S->steps_per_launch);
+  // without whole exchange groups per CTA the exchange is a separate launch
+  // after each server iteration, so the iteration must be one interval
+  if ((mc->flags & GD_MC_EXCHANGE) && 32 % mc->n_tmp != 0 &&
+      mc->steps_per_exchange != S->steps_per_launch)
+    return fail(GD_EINVAL, "n_tmp=%d needs steps_per_exchange == %d (the server's steps per "
+                "launch)", mc->n_tmp, S->steps_per_launch);
+  if (mc->steps_total < S->steps_per_launch || mc->steps_total % S->steps_per_launch != 0)
+    return fail(GD_EINVAL, "steps_total %d is not a multiple of %d", mc->steps_total,
+                S->steps_per_launch);
+  auto r = std::make_unique<Req>();
+  try {
+    GD_TRY(copy_request(S, protein_id, cx, mc, r.get()));
+  } catch (const std::bad_alloc &) {
+    return fail(GD_ENOMEM, "host allocation");
+  }
+  GD_TRY(gd_complex_validate(&r->cx));
+  std::lock_guard<std::mutex> g(S->mu);
+  if (S->protein_bytes + r->bytes > S->budget)
+    return fail(GD_EBUDGET, "request needs %zu bytes; budget %zu, proteins hold %zu", r->bytes,
+                S->budget, S->protein_bytes);
+  r->id = S->next_id++;
+  r->t_submit = Clock::now();
+  *req_id = r->id;
+  S->queue.push_back(r.get());
+  S->reqs[r->id] = std::move(r);
+  S->cv.notify_all();
+  return GD_OK;
+}
+
+static gd_status take_result(gd_server *S, std::unordered_map<uint64_t, std::unique_ptr<Req>>::iterator it,
+                             gd_mc_log *log) {
+  Req *r = it->second.get();
+  gd_status st = GD_OK;
+  if (r->state == RQ_DONE) {
+    if (log) {
+      const size_t n = (size_t)r->n_rep;
+      if (log->energy) std::memcpy(log->energy, r->energy.data(), n * GD_NTERM * 4);
+      if (log->movematrix) std::memcpy(log->movematrix, r->movematrix.data(), n * 24);
+      if (log->acs_mc) std::memcpy(log->acs_mc, r->acs.data(), n * 4);
+      if (log->idx_tmp) std::memcpy(log->idx_tmp, r->idx.data(), n * 4);
+      if (log->acs_temp_exchg) std::memcpy(log->acs_temp_exchg, r->acx.data(), r->acx.size() * 4);
+      log->ac_mc = 0;
+      for (int v : r->acs) log->ac_mc += v;
+      log->ac_temp_exchg = 0;
+      for (int v : r->acx) log->ac_temp_exchg += v;
+      log->t_wall = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+      log->t_compute = std::chrono::duration<double>(r->t_done - r->t_start).count();
+    }
+  } else if (r->state == RQ_CANCELLED) {
+    st = fail(GD_ECANCELLED, "request %llu was cancelled", (unsigned long long)r->id);
+  } else {
+    st = r->err != GD_OK ? r->err : GD_ECUDA;
+  }
+  S->reqs.erase(it);
+  return st;
+}
+
+extern "C" gd_status gd_server_poll(gd_server *S, uint64_t req_id, gd_mc_log *log) {
+  if (!S) return fail(GD_EINVAL, "server NULL");
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->reqs.find(req_id);
+  if (it == S->reqs.end()) return fail(GD_ENOTFOUND, "no request %llu", (unsigned long long)req_id);
+  const ReqState st = it->second->state;
+  if (st == RQ_QUEUED || st == RQ_ACTIVE) return GD_EAGAIN;
+  return take_result(S, it, log);
+}
+
+extern "C" gd_status gd_server_wait(gd_server *S, uint64_t req_id, int timeout_ms,
+                                    gd_mc_log *log) {
+  if (!S) return fail(GD_EINVAL, "server NULL");
+  std::unique_lock<std::mutex> lk(S->mu);
+  const auto deadline = Clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+  for (;;) {
+    auto it = S->reqs.find(req_id);
+    if (it == S->reqs.end())
+      return fail(GD_ENOTFOUND, "no request %llu", (unsigned long long)req_id);
+    const ReqState st = it->second->state;
+    if (st != RQ_QUEUED && st != RQ_ACTIVE) return take_result(S, it, log);
+    if (S->done_cv.wait_until(lk, deadline) == std::cv_status::timeout) {
+      auto it2 = S->reqs.find(req_id);
+      if (it2 != S->reqs.end() &&
+          (it2->second->state == RQ_QUEUED || it2->second->state == RQ_ACTIVE))
+        return fail(GD_ETIMEDOUT, "request %llu not finished after %d ms",
+                    (unsigned long long)req_id, timeout_ms);
+    }
+  }
+}
+
+extern "C" gd_status gd_server_cancel(gd_server *S, uint64_t req_id) {
+  if (!S) return fail(GD_EINVAL, "server NULL");
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->reqs.find(req_id);
+  if (it == S->reqs.end()) return fail(GD_ENOTFOUND, "no request %llu", (unsigned long long)req_id);
+  it->second->cancel = true;
+  S->cv.notify_all();
+  return GD_OK;
+}
+
+extern "C" gd_status gd_server_get_stats(gd_server *S, gd_server_stats *out) {
+  if (!S || !out) return fail(GD_EINVAL, "gd_server_get_stats: NULL argument");
+  std::lock_guard<std::mutex> g(S->mu);
+  out->queued = (int)S->queue.size();
+  out->active = (int)S->active.size();
+  out->completed = S->n_done;
+  out->iterations = S->n_iter;
+  out->launches = S->n_launch;
+  out->bytes_in_use = S->bytes_in_use + S->protein_bytes;
+  out->busy_s = S->busy_s;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_server_destroy(gd_server *S) {
+  if (!S) return GD_OK;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    S->stop = true;
+    S->cv.notify_all();
+  }
+  if (S->th.joinable()) S->th.join();
+  cudaSetDevice(S->ctx->device);
+  for (Req *r : S->active) release_device(S, r);
+  cudaStreamSynchronize(S->ctx->stream);
+  for (auto &p : S->proteins) dcx_release(p->dcx);
+  if (S->d_items) cudaFree(S->d_items);
+  if (S->d_cta) cudaFree(S->d_cta);
+  if (S->d_groups) cudaFree(S->d_groups);
+  if (S->ev) cudaEventDestroy(S->ev);
+  ctx_release(S->ctx);
+  delete S;
+  return GD_OK;
+}

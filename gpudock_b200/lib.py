@@ -52,6 +52,15 @@ def _declare(lib):
         "gd_batch_set_profiling": ([P, i32], i32),
         "gd_batch_kernel_times": ([P, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int)], i32),
+        "gd_server_create": ([i32, C.c_size_t, i32, i32, C.POINTER(P)], i32),
+        "gd_server_add_protein": ([P, C.POINTER(abi.GdComplex), C.POINTER(C.c_int)], i32),
+        "gd_server_submit": ([P, i32, C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams),
+                              C.POINTER(C.c_uint64)], i32),
+        "gd_server_poll": ([P, C.c_uint64, C.POINTER(abi.GdMcLog)], i32),
+        "gd_server_wait": ([P, C.c_uint64, i32, C.POINTER(abi.GdMcLog)], i32),
+        "gd_server_cancel": ([P, C.c_uint64], i32),
+        "gd_server_get_stats": ([P, C.POINTER(abi.GdServerStats)], i32),
+        "gd_server_destroy": ([P], i32),
         "gd_complex_free": ([P], i32),
         "gd_complex_device_bytes": ([P], C.c_size_t),
         "gd_energy_poses_dev": ([P, P, i32, i32, i32, P, P, P], i32),
@@ -329,6 +338,73 @@ class Batch:
     def close(self):
         if self.h:
             self.ctx._lib.gd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving form (gd_server): resident proteins, a request queue with
+    HBM-budget admission and continuous batching on a scheduler thread."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 120 << 30, max_active: int = 0,
+                 steps_per_launch: int = 10):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.gd_server_create(device, int(hbm_budget_bytes), int(max_active),
+                                         int(steps_per_launch), C.byref(h)), "gd_server_create")
+        self.h = h
+        self._pending = {}  # request id -> (McLogBuffers, complex, params, keep-alive)
+
+    def add_protein(self, cx: abi.Complex) -> int:
+        pid = C.c_int()
+        check(self._lib.gd_server_add_protein(self.h, C.byref(cx.struct()), C.byref(pid)),
+              "gd_server_add_protein")
+        return pid.value
+
+    def submit(self, protein_id: int, cx: abi.Complex, steps_total: int, steps_per_exchange: int,
+               minus_beta, n_prt: int, **kw) -> int:
+        params, mb = abi.mc_params(steps_total, steps_per_exchange, minus_beta, **kw)
+        rid = C.c_uint64()
+        check(self._lib.gd_server_submit(self.h, protein_id, C.byref(cx.struct()),
+                                         C.byref(params), C.byref(rid)), "gd_server_submit")
+        n_rep = n_prt * cx.n_lig * len(mb)
+        self._pending[rid.value] = abi.McLogBuffers(n_rep, len(mb))
+        return rid.value
+
+    def poll(self, rid: int):
+        """None while running; the results when done (raises on failure)."""
+        buf = self._pending[rid]
+        st = self._lib.gd_server_poll(self.h, C.c_uint64(rid), C.byref(buf.log))
+        if st == abi.GD_EAGAIN:
+            return None
+        del self._pending[rid]
+        check(st, "gd_server_poll")
+        return buf
+
+    def wait(self, rid: int, timeout_ms: int = 600000):
+        buf = self._pending[rid]
+        st = self._lib.gd_server_wait(self.h, C.c_uint64(rid), int(timeout_ms), C.byref(buf.log))
+        if st != abi.GD_ETIMEDOUT:
+            del self._pending[rid]
+        check(st, "gd_server_wait")
+        return buf
+
+    def cancel(self, rid: int):
+        check(self._lib.gd_server_cancel(self.h, C.c_uint64(rid)), "gd_server_cancel")
+
+    def stats(self) -> abi.GdServerStats:
+        s = abi.GdServerStats()
+        check(self._lib.gd_server_get_stats(self.h, C.byref(s)), "gd_server_get_stats")
+        return s
+
+    def close(self):
+        if self.h:
+            self._lib.gd_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

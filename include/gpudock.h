@@ -362,6 +362,47 @@ gd_status gd_batch_kernel_times(gd_batch *batch, double *mc_ms, int *mc_launches
                                 double *exch_ms, int *exch_launches);
 
 /* ------------------------------------------------------------------------ */
+/* Serving form: a request loop with continuous batching.  Proteins are     */
+/* uploaded once and stay resident; requests (a ligand ensemble + pocket    */
+/* template + MC parameters against a resident protein) are copied at       */
+/* submit, admitted by a scheduler thread while the HBM budget and the      */
+/* slot count allow, and advanced together steps_per_launch MC steps per    */
+/* iteration, each with its own step counter, state and random stream, so  */
+/* a request's result does not depend on what else is running.              */
+/* ------------------------------------------------------------------------ */
+typedef struct gd_server gd_server;
+
+typedef struct gd_server_stats {
+  int queued;               /* waiting for admission                        */
+  int active;               /* admitted, running                            */
+  uint64_t completed;       /* finished successfully                        */
+  uint64_t iterations;      /* scheduler iterations                         */
+  uint64_t launches;        /* kernel launches issued                       */
+  size_t bytes_in_use;      /* device bytes held (proteins + requests)      */
+  double busy_s;            /* seconds the scheduler spent in iterations    */
+} gd_server_stats;
+
+/* max_active <= 0 means two requests per SM. */
+gd_status gd_server_create(int device, size_t hbm_budget_bytes, int max_active,
+                           int steps_per_launch, gd_server **out);
+/* Makes the protein (all conformations) of cx resident; returns its id. */
+gd_status gd_server_add_protein(gd_server *srv, const gd_complex *cx, int *protein_id);
+/* Copies the request (cx->prt is ignored: the resident protein is used).
+ * GD_EBUDGET when it can never fit the budget. */
+gd_status gd_server_submit(gd_server *srv, int protein_id, const gd_complex *cx,
+                           const gd_mc_params *mc, uint64_t *req_id);
+/* GD_EAGAIN while queued or running; GD_OK with the results (t_wall = latency
+ * from submit, t_compute = time since admission) and the request released;
+ * GD_ECANCELLED / the failure status otherwise. */
+gd_status gd_server_poll(gd_server *srv, uint64_t req_id, gd_mc_log *log);
+/* As poll, blocking up to timeout_ms (GD_ETIMEDOUT after). */
+gd_status gd_server_wait(gd_server *srv, uint64_t req_id, int timeout_ms,
+                         gd_mc_log *log);
+gd_status gd_server_cancel(gd_server *srv, uint64_t req_id);
+gd_status gd_server_get_stats(gd_server *srv, gd_server_stats *out);
+gd_status gd_server_destroy(gd_server *srv);
+
+/* ------------------------------------------------------------------------ */
 /* Building blocks exposed for testing: the Metropolis and exchange rules   */
 /* on given energies, the counter-based RNG and the decision exp.           */
 /* ------------------------------------------------------------------------ */

@@ -115,3 +115,22 @@ def test_energy_invalid_inputs(ctx):
     with pytest.raises(lib.GdError) as e:
         lib.DeviceComplex(ctx, bad)
     assert e.value.status == abi.GD_EINVAL
+
+
+def test_golden_line_on_gpu(ctx):
+    """The 1a07C1 sample complex (tables from the reference's own loaders):
+    the kernel reproduces the published initial-energy line
+    (SimilarityMatirxGen/data/report:21-22) to its four decimals, through the
+    MonteCarlo_Init_d path (move-away pose, forced accept)."""
+    from tests.golden_fixture import golden_lines, load_complex
+    cx, _, _ = load_complex("smg")
+    g = np.array(golden_lines()["report"])
+    d = lib.DeviceComplex(ctx, cx)
+    pose = (np.float32([0.02, 0.02, 0.02, 0.08, 0.08, 0.08]) * np.float32(44.5)).reshape(1, 6)
+    terms, raw = d.energy_poses(pose)
+    assert np.allclose(np.round(terms[0].astype(np.float64), 4), g, atol=1.01e-4), terms[0]
+    _, mb = lib.set_temperature(1, 0.044, 0.036)
+    r = lib.Remc(d, 10, 10, mb, flags=abi.MC_MOVE_AWAY)
+    r.init()
+    out = r.read()
+    assert np.allclose(np.round(out.energy[0].astype(np.float64), 4), g, atol=1.01e-4)
