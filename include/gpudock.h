@@ -263,6 +263,33 @@ gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *dcx, int prt_conf,
                           int lig_conf, int n_pose, const float *poses,
                           float *terms, double *raw);
 
+/* Same computation and results as gd_energy_poses (host buffers), without
+ * allocating any device memory. It has no counterpart in the reference.
+ *
+ * Who needs it: a caller that has handed its spare device memory to another
+ * allocator (the serving form's HBM budget, a framework's caching
+ * allocator) can see even a small cudaMalloc/cudaMallocAsync fail, and a
+ * caller may want no allocator call at all on its scoring path. This entry
+ * point stages poses, results and the launch descriptor in one fixed
+ * device array compiled into the library (about 2.2 MB per device) instead.
+ *
+ * Limit: n_pose <= GD_NOALLOC_MAX_POSES; larger calls return GD_EINVAL
+ * before anything runs (split them, or use gd_energy_poses).
+ * Set-up: the first call on a device looks up the array's address on that
+ * device (it must be current; the call makes ctx's device current), so make
+ * that first call before any stream capture.
+ * Nothing in the array has to start at zero: each call writes what the kernel
+ * reads before the launch.
+ * Overlapping calls race: there is one array per device, shared by every
+ * context and thread of the process, and calls are not serialised. Do not
+ * let two calls on the same device run at the same time. Each call waits
+ * for its own results before it returns. */
+#define GD_NOALLOC_MAX_POSES 16384
+gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *dcx,
+                                  int prt_conf, int lig_conf, int n_pose,
+                                  const float *poses, float *terms,
+                                  double *raw);
+
 /* ------------------------------------------------------------------------ */
 /* Replica-exchange Monte Carlo                                             */
 /* ------------------------------------------------------------------------ */
