@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the plain / batched / served / pose-sweep measurements")
     return ap.parse_args()
 
 
@@ -160,6 +162,171 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
                       f"{'-march=native' if native else 'x86-64'} OpenMP build)"}
 
 
+def _event_ms(stream, fn):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def form_plain(ctx, stream, seed, flush):
+    """Plain form of the single-complex workload: 1,500 points x 24 atoms,
+    8 temperatures (8 replicas, one CTA), exchange every 10 steps."""
+    from gpudock_b200 import lib
+    w, cx, mb = build_workload("plain_1500x24", seed)
+    n_rep = cx.n_prt * cx.n_lig * w.n_tmp
+    d = lib.DeviceComplex(ctx, cx)
+    steps = 200
+    r = lib.Remc(d, 4 * steps, w.steps_per_exchange, mb, w.move_scale, seed=seed)
+    r.init()
+    r.run(steps)
+    flush.fill_(1)
+    ms = _event_ms(stream, lambda: r.run(steps))
+    r.read()
+    r.close()
+    d.close()
+    return {"workload": w.name, "n_rep": n_rep, "mc_steps": steps,
+            "value": n_rep * steps / (ms * 1e-3), "unit": "replica-MC-steps/s",
+            "ms_per_mc_step": ms / steps}
+
+
+def form_batched(ctx, stream, seed, flush, n_steps=50):
+    """Batched form: 512 ligands of 12..96 atoms x 4 conformations x 8
+    temperatures (16,384 replicas) against one 6,000-point protein with 4
+    conformations, exchange every 10 steps; launch shapes autotuned per
+    ligand-size bucket; timed over n_steps MC steps (a sample of the 3,000)."""
+    import dataclasses
+    from gpudock_b200 import abi, lib, synth
+    w = synth.WORKLOADS["batched_512"]
+    raw, _, _ = synth.default_ff()
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    prt = synth.make_protein(rng, w.spec, 9.0, raw)
+    lo, hi = w.extra["lna_range"]
+    lnas = rng.integers(lo, hi + 1, size=w.extra["n_ligand"])
+    cxs = [synth.make_complex(dataclasses.replace(w.spec, lna=int(n), n_prt=w.spec.n_prt),
+                              seed=seed + 100 + i, protein=prt) for i, n in enumerate(lnas)]
+    _, mb = synth.temperatures(w)
+    base = lib.DeviceComplex(ctx, cxs[0])
+    dcxs = [lib.DeviceComplex(ctx, cx, share=base, prt_conf0=i % w.spec.n_prt, n_prt=1)
+            for i, cx in enumerate(cxs)]
+    t0 = time.perf_counter()
+    tuned = lib.autotune_buckets(dcxs)
+    tune_s = time.perf_counter() - t0
+    params = [abi.mc_params(w.steps, w.steps_per_exchange, mb, w.move_scale, seed=seed,
+                            stream_id=i, flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY)
+              for i in range(len(dcxs))]
+    b = lib.Batch(ctx, dcxs, params)
+    b.init()
+    b.run(2 * w.steps_per_exchange)
+    flush.fill_(2)
+    launches0 = ctx.launches
+    ms = _event_ms(stream, lambda: b.run(n_steps))
+    launches = ctx.launches - launches0
+    b.set_profiling(True)
+    b.run(n_steps)
+    mc_ms, mc_n, ex_ms, ex_n = b.kernel_times()
+    b.set_profiling(False)
+    pairs = sum(4 * w.n_tmp * int(n) for n in lnas) * w.spec.pnp * n_steps
+    out = {"workload": w.name, "n_rep": b.n_rep, "n_ligand": len(cxs),
+           "lna_range": [int(lnas.min()), int(lnas.max())], "mc_steps_timed": n_steps,
+           "value": b.n_rep * n_steps / (ms * 1e-3), "unit": "replica-MC-steps/s",
+           "ms_per_mc_step": ms / n_steps, "launch_shapes": b.n_shapes,
+           "gpu_launches": launches,
+           "fp32_tflops": FLOP_PER_PAIR * pairs / (mc_ms * 1e-3) / 1e12 if mc_ms else None,
+           "autotune_s": tune_s,
+           "tiles": {f"lna<={k[0]},tiles={k[1]}": list(v[0]) for k, v in tuned.items()}}
+    b.close()
+    for d in dcxs:
+        d.close()
+    base.close()
+    return out
+
+
+def form_served(seed, rate=50.0, n_request=300, steps=2000, budget_gb=120):
+    """Serving form: Poisson arrivals at `rate` req/s; ligand sizes log-normal
+    (median 30, clipped to 8..120); each request 4 ligand conformations x 8
+    temperatures (32 replicas) x `steps` MC steps against one of 4 resident
+    proteins (2,000 / 4,000 / 7,000 / 10,000 points); admission by an HBM
+    budget.  Latency = submit -> result, measured by the server."""
+    import dataclasses
+    from gpudock_b200 import abi, lib, synth
+    w = synth.WORKLOADS["serving"]
+    raw, _, _ = synth.default_ff()
+    rng = np.random.Generator(np.random.PCG64(seed + 2))
+    prots = [synth.make_protein(rng, dataclasses.replace(w.spec, pnp=p), 10.0, raw)
+             for p in w.extra["proteins"]]
+    lo, hi = w.extra["lna_clip"]
+    lnas = np.clip(np.round(np.exp(rng.normal(np.log(w.extra["lna_median"]), 0.5,
+                                              n_request))), lo, hi).astype(int)
+    which = rng.integers(0, len(prots), n_request)
+    gaps = rng.exponential(1.0 / rate, n_request)
+    cxs = [synth.make_complex(dataclasses.replace(w.spec, lna=int(n),
+                                                  pnp=w.extra["proteins"][k]),
+                              seed=seed + 1000 + i, protein=prots[k])
+           for i, (n, k) in enumerate(zip(lnas, which))]
+    _, mb = synth.temperatures(w)
+    srv = lib.Server(0, hbm_budget_bytes=int(budget_gb) << 30, max_active=0,
+                     steps_per_launch=w.steps_per_exchange * 10)
+    pids = []
+    for k in range(len(prots)):
+        first = next(i for i in range(n_request) if which[i] == k) if (which == k).any() else None
+        pids.append(srv.add_protein(cxs[first]) if first is not None else None)
+    ids = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for i, cx in enumerate(cxs):
+        t_next += gaps[i]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(srv.submit(pids[which[i]], cx, steps, w.steps_per_exchange, mb, n_prt=1,
+                              seed=seed, stream_id=i, flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY))
+    lat = []
+    for rid in ids:
+        lat.append(srv.wait(rid, timeout_ms=900000).log.t_wall)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.asarray(lat)
+    n_rep = 32
+    return {"workload": w.name, "n_request": n_request, "rate_req_s": rate,
+            "mc_steps": steps, "replicas_per_request": n_rep,
+            "value": n_request * n_rep * steps / wall, "unit": "replica-MC-steps/s",
+            "requests_per_s": n_request / wall,
+            "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "busy_s": st.busy_s, "launches": st.launches,
+            "sample": f"{n_request} of the 10,000-request trace at {rate:g} req/s"}
+
+
+def form_poses(ctx, stream, seed, n_pose=1 << 20):
+    """Energy-only sweep: n_pose random rigid poses of a 48-atom ligand against
+    proteins of 2,000 / 4,000 / 8,000 / 16,000 points (pose-energies/s)."""
+    import dataclasses
+    import torch
+    from gpudock_b200 import lib, synth
+    w = synth.WORKLOADS["poses_48"]
+    rng = np.random.default_rng(seed + 3)
+    poses = torch.from_numpy(synth.random_poses(rng, n_pose, box=w.extra["box"])).cuda()
+    terms = torch.empty((n_pose, 10), dtype=torch.float32, device="cuda")
+    out = {}
+    for pnp in w.extra["pnp_sweep"]:
+        cx = synth.make_complex(dataclasses.replace(w.spec, pnp=pnp), seed=seed + pnp)
+        d = lib.DeviceComplex(ctx, cx)
+        tile, _ = d.autotune()
+        run = lambda: d.energy_poses_dev(n_pose, poses.data_ptr(), terms.data_ptr())
+        run()
+        ms = _event_ms(stream, run)
+        out[str(pnp)] = {"value": n_pose / (ms * 1e-3), "unit": "pose-energies/s",
+                         "fp32_tflops": FLOP_PER_PAIR * n_pose * cx.lna * pnp / (ms * 1e-3)
+                         / 1e12, "tile": list(tile)}
+        d.close()
+    return {"workload": w.name, "n_pose": n_pose, "by_protein_points": out}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU path (oracle port) on all cores."""
     ws, rank, _ = dist_env()
@@ -234,6 +401,7 @@ def main():
     torch.cuda.set_stream(stream)
     ctx = lib.Context(local, stream.cuda_stream)
     dcx = lib.DeviceComplex(ctx, cx)
+    tile, _ = dcx.autotune()  # launch shape of this size class, kept in ctx
     total_steps = spe * (args.warmup + args.steps + 2)
     remc = lib.Remc(dcx, total_steps, spe, mb, w.move_scale, seed=args.seed + rank)
     remc.init()
@@ -302,6 +470,18 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "gd_run: upload + init + 20 MC steps + exchange + read-back per step"}
 
+    forms = None
+    if ws == 1 and not args.no_forms:
+        forms = {}
+        for name, fn in (("plain", lambda: form_plain(ctx, stream, args.seed, flush)),
+                         ("batched", lambda: form_batched(ctx, stream, args.seed, flush)),
+                         ("poses", lambda: form_poses(ctx, stream, args.seed)),
+                         ("served", lambda: form_served(args.seed))):
+            try:
+                forms[name] = fn()
+            except Exception as exc:  # reported, not fatal
+                forms[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
@@ -318,6 +498,7 @@ def main():
             "config": {"workload": w.name, "n_rep": n_rep, "n_prt": cx.n_prt,
                        "n_lig": cx.n_lig, "n_tmp": w.n_tmp, "lna": cx.lna, "pnp": cx.pnp,
                        "steps_per_exchange": spe, "step": "one exchange interval",
+                       "tile_A_P_NA": list(tile),
                        "l2": "flushed (256 MiB write) before every step",
                        "parallelism": f"replicas, {ws} independent ensemble(s)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
@@ -328,6 +509,7 @@ def main():
                          "peak_source": "measured live: FP32 FMA probe kernel on this GPU",
                          "exchange_kernel_ms": ex_ms / max(ex_n, 1)},
             "cpu_baseline": cpu,
+            "forms": forms,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
             "clocks": clk,

@@ -80,15 +80,18 @@ static bool fits_resident(const KTables &T, const Tile &t) {
          dock_smem_bytes(t.A, t.P, t.NA, n_tiles) <= 227 * 1024;
 }
 
+int lna_bucket(int lna) { return std::min(((lna + 7) / 8) * 8, MAX_LNA); }
+
 Tile tile_for(gd_ctx *ctx, const KTables &T) {
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  const int hi = lna_bucket(T.lna);
   {
     std::lock_guard<std::mutex> g(ctx->tile_mu);
-    auto it = ctx->tiles.find({T.lna, n_tiles});
+    auto it = ctx->tiles.find({hi, n_tiles});
     if (it != ctx->tiles.end()) return it->second;
   }
-  Tile t = default_tile(T.lna, true);
-  if (!fits_resident(T, t)) t = default_tile(T.lna, false);
+  Tile t = default_tile(hi, true);
+  if (!fits_resident(T, t)) t = default_tile(hi, false);
   return t;
 }
 
@@ -96,10 +99,46 @@ void ctx_retain(gd_ctx *c) {
   if (c) c->refs++;
 }
 
+gd_status fork_streams(gd_ctx *c, int n, cudaStream_t *out) {
+  n = std::max(1, std::min(n, kMaxSide));
+  out[0] = c->stream;
+  if (n == 1) return GD_OK;
+  if (!c->forked) GD_CUDA(cudaEventCreateWithFlags(&c->forked, cudaEventDisableTiming));
+  while ((int)c->side.size() < n - 1) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    GD_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    c->side.push_back(s);
+    GD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->side_done.push_back(e);
+  }
+  GD_CUDA(cudaEventRecord(c->forked, c->stream));
+  for (int k = 1; k < n; ++k) {
+    GD_CUDA(cudaStreamWaitEvent(c->side[k - 1], c->forked, 0));
+    out[k] = c->side[k - 1];
+  }
+  return GD_OK;
+}
+
+gd_status join_streams(gd_ctx *c, int n) {
+  n = std::max(1, std::min(n, kMaxSide));
+  for (int k = 1; k < n; ++k) {
+    GD_CUDA(cudaEventRecord(c->side_done[k - 1], c->side[k - 1]));
+    GD_CUDA(cudaStreamWaitEvent(c->stream, c->side_done[k - 1], 0));
+  }
+  return GD_OK;
+}
+
 void ctx_release(gd_ctx *c) {
   if (!c || --c->refs > 0) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  for (cudaStream_t s : c->side) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : c->side_done) cudaEventDestroy(e);
+  if (c->forked) cudaEventDestroy(c->forked);
   cudaFree(c->d_err);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -620,7 +659,7 @@ extern "C" gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *d, gd_tile *bes
                                  double *best_ms) {
   if (!ctx || !d) return fail(GD_EINVAL, "gd_autotune: NULL handle");
   GD_CUDA(cudaSetDevice(ctx->device));
-  const int lna = d->T.lna;
+  const int lna = lna_bucket(d->T.lna);  // the tile must cover the whole size bucket
   const int n_pose = 32 * ctx->n_sm;
   std::vector<float> hp((size_t)n_pose * 6);
   uint32_t s = 12345u;
@@ -695,11 +734,12 @@ extern "C" gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_til
   t.A = tile->atom_groups;
   t.P = tile->tile_groups;
   t.NA = tile->atoms_per_warp;
-  if (!t.valid() || t.A * t.P > MAX_WARPS || round_na(t.NA) != t.NA || t.A * t.NA < lna)
+  if (!t.valid() || t.A * t.P > MAX_WARPS || round_na(t.NA) != t.NA ||
+      t.A * t.NA < lna_bucket(lna))
     return fail(GD_EINVAL, "tile %dx%d with %d atoms per warp does not cover %d atoms", t.A, t.P,
                 t.NA, lna);
   std::lock_guard<std::mutex> g(ctx->tile_mu);
-  ctx->tiles[{lna, (pnp + TILE_PTS - 1) / TILE_PTS}] = t;
+  ctx->tiles[{lna_bucket(lna), (pnp + TILE_PTS - 1) / TILE_PTS}] = t;
   return GD_OK;
 }
 

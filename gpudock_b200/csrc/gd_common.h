@@ -62,9 +62,13 @@ struct gd_ctx {
   uint64_t launches = 0;
   int n_sm = 148;
   std::atomic<int> refs{1};
-  // autotuned launch shapes keyed by (ligand atoms, protein tiles)
+  // autotuned launch shapes keyed by (ligand-size bucket, protein tiles)
   std::mutex tile_mu;
   std::map<std::pair<int, int>, gd::Tile> tiles;
+  // side streams: launches of different shapes run side by side on them
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_done;
+  cudaEvent_t forked = nullptr;
 };
 
 struct gd_dcomplex {
@@ -82,5 +86,19 @@ void ctx_release(gd_ctx *c);
 void dcx_retain(gd_dcomplex *d);
 void dcx_release(gd_dcomplex *d);
 gd_status ctx_check(gd_ctx *c);
+// Ligand-size bucket: sizes are rounded up to a multiple of 8 atoms; launch
+// shapes are chosen (and autotuned) per bucket and cover its largest size.
+int lna_bucket(int lna);
 Tile tile_for(gd_ctx *ctx, const KTables &T);
+
+// Launches of different shapes (one per launch plan) are independent; each
+// kernel holds one CTA per SM, so a plan with fewer CTAs than SMs leaves the
+// rest idle unless the next plan runs beside it.  fork_streams returns n
+// streams (n <= kMaxSide; the first is ctx->stream) that start after the work
+// already queued on ctx->stream; join_streams makes ctx->stream wait for all
+// of them.  Both work inside a stream capture, which turns the plans into
+// parallel graph branches.
+constexpr int kMaxSide = 8;
+gd_status fork_streams(gd_ctx *c, int n, cudaStream_t *out);
+gd_status join_streams(gd_ctx *c, int n);
 }  // namespace gd

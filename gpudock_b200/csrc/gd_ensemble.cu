@@ -33,6 +33,7 @@ namespace {
 
 struct Plan {
   Tile tile;
+  double cost = 0.0;  // sum over its CTAs of ligand atoms x protein points
   int n_stages = 0, resident = 0, group_major = 0, fused = 0, grid = 0;
   int *d_cta_item = nullptr, *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
 };
@@ -232,6 +233,7 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
       ci.push_back(std::get<1>(c));
       c0.push_back(std::get<2>(c));
       cn.push_back(std::get<3>(c));
+      pl.cost += std::get<0>(c);
     }
     pl.grid = (int)ci.size();
     GD_TRY(dcopy(E, &pl.d_cta_item, ci));
@@ -239,8 +241,18 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     GD_TRY(dcopy(E, &pl.d_cta_nrep, cn));
     E.plans.push_back(pl);
   }
+  // costliest plans are issued first, so they start first on the SMs
+  std::stable_sort(E.plans.begin(), E.plans.end(),
+                   [](const Plan &a, const Plan &b) { return a.cost > b.cost; });
   E.n_groups = (int)groups.size();
   if (E.n_groups) GD_TRY(dcopy(E, &E.d_groups, groups));
+  {
+    // create the side streams now, outside any later stream capture
+    cudaStream_t ss[kMaxSide];
+    const int ns = std::min((int)E.plans.size(), kMaxSide);
+    GD_TRY(fork_streams(ctx, ns, ss));
+    GD_TRY(join_streams(ctx, ns));
+  }
   GD_CUDA(cudaEventCreate(&E.ev0));
   GD_CUDA(cudaEventCreate(&E.ev1));
   GD_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -274,18 +286,33 @@ gd_status mark(Ens &E, int kind) {
   return GD_OK;
 }
 
+// One launch per plan, the plans side by side on the context's side streams
+// (joined back into ctx->stream).  Profiling brackets the whole group.
+gd_status launch_plans(Ens &E, int mode, int step0, int n_steps, bool device_step) {
+  const int n = std::min((int)E.plans.size(), kMaxSide);
+  cudaStream_t ss[kMaxSide];
+  if (E.profile && mode == KMODE_REMC) GD_TRY(mark(E, 0));
+  GD_TRY(fork_streams(E.ctx, n, ss));
+  for (size_t k = 0; k < E.plans.size(); ++k) {
+    const Plan &pl = E.plans[k];
+    KRun R = run_desc(E, pl, mode);
+    R.step0 = step0;
+    R.n_steps = n_steps;
+    R.step_ptr = device_step ? E.d_step : nullptr;
+    GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, ss[k % n]));
+    E.ctx->launches += 1;
+  }
+  GD_TRY(join_streams(E.ctx, n));
+  if (E.profile && mode == KMODE_REMC) GD_TRY(mark(E, 0));
+  return GD_OK;
+}
+
 gd_status ens_init(Ens &E) {
   GD_CUDA(cudaSetDevice(E.ctx->device));
   cudaStream_t s = E.ctx->stream;
   GD_CUDA(cudaMemsetAsync(E.acs_exchg, 0, sizeof(int) * MAX_TMP * E.items.size(), s));
   GD_CUDA(cudaMemsetAsync(E.d_step, 0, sizeof(int), s));
-  for (const Plan &pl : E.plans) {
-    KRun R = run_desc(E, pl, KMODE_INIT);
-    R.step0 = 0;
-    R.n_steps = 1;
-    GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
-    E.ctx->launches += 1;
-  }
+  GD_TRY(launch_plans(E, KMODE_INIT, 0, 1, false));
   E.step = 0;
   E.t_compute = 0.0;
   return GD_OK;
@@ -297,16 +324,7 @@ gd_status ens_enqueue(Ens &E, int n_steps, bool device_step) {
   cudaStream_t s = E.ctx->stream;
   if (E.all_fused) {
     // exchanges happen inside the kernel: one launch per plan for the run
-    for (const Plan &pl : E.plans) {
-      KRun R = run_desc(E, pl, KMODE_REMC);
-      R.step0 = E.step;
-      R.n_steps = n_steps;
-      R.step_ptr = device_step ? E.d_step : nullptr;
-      if (E.profile) GD_TRY(mark(E, 0));
-      GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
-      if (E.profile) GD_TRY(mark(E, 0));
-      E.ctx->launches += 1;
-    }
+    GD_TRY(launch_plans(E, KMODE_REMC, E.step, n_steps, device_step));
     if (device_step) {
       GD_CUDA(launch_advance(E.d_step, n_steps, s));
       E.ctx->launches += 1;
@@ -314,16 +332,7 @@ gd_status ens_enqueue(Ens &E, int n_steps, bool device_step) {
     return GD_OK;
   }
   for (int s0 = E.step; s0 < E.step + n_steps; s0 += E.spe) {
-    for (const Plan &pl : E.plans) {
-      KRun R = run_desc(E, pl, KMODE_REMC);
-      R.step0 = s0;
-      R.n_steps = E.spe;
-      R.step_ptr = device_step ? E.d_step : nullptr;
-      if (E.profile) GD_TRY(mark(E, 0));
-      GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, s));
-      if (E.profile) GD_TRY(mark(E, 0));
-      E.ctx->launches += 1;
-    }
+    GD_TRY(launch_plans(E, KMODE_REMC, s0, E.spe, device_step));
     if (E.n_groups) {
       if (E.profile) GD_TRY(mark(E, 1));
       GD_CUDA(launch_exchange(E.d_items, E.d_groups, E.n_groups, E.spe, s0,

@@ -267,7 +267,20 @@ gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n
   if (!groups.empty())
     GD_CUDA(cudaMemcpyAsync(S->d_groups, groups.data(), groups.size() * sizeof(KGroup),
                             cudaMemcpyHostToDevice, s));
-  for (auto &lp : launches) {
+  // the shapes run side by side on side streams, costliest issued first
+  auto plan_cost = [](const ShapePlan *p) {
+    double c = 0.0;
+    for (const auto &t : p->ctas) c += std::get<0>(t);
+    return c;
+  };
+  std::stable_sort(launches.begin(), launches.end(), [&](const auto &a, const auto &b) {
+    return plan_cost(a.first) > plan_cost(b.first);
+  });
+  const int n_side = std::min((int)launches.size(), kMaxSide);
+  cudaStream_t ss[kMaxSide];
+  GD_TRY(fork_streams(S->ctx, n_side, ss));
+  for (size_t k = 0; k < launches.size(); ++k) {
+    const auto &lp = launches[k];
     const ShapePlan &pl = *lp.first;
     KRun R{};
     R.mode = mode;
@@ -286,10 +299,11 @@ gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n
     R.n_steps = n_steps;
     R.item_step = 1;
     R.err = S->ctx->d_err;
-    GD_CUDA(launch_dock(R, pl.tile.NA, (int)pl.ctas.size(), s));
+    GD_CUDA(launch_dock(R, pl.tile.NA, (int)pl.ctas.size(), ss[k % n_side]));
     S->ctx->launches += 1;
     S->n_launch += 1;
   }
+  GD_TRY(join_streams(S->ctx, n_side));
   if (!groups.empty()) {
     GD_CUDA(launch_exchange(S->d_items, S->d_groups, (int)groups.size(), S->steps_per_launch, -1,
                             nullptr, s));

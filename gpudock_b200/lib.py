@@ -202,6 +202,11 @@ class DeviceComplex:
         return (t.atom_groups, t.tile_groups, t.atoms_per_warp), ms.value
 
     @property
+    def size_class(self):
+        """(ligand-size bucket, protein tiles): the key of the context's shape cache."""
+        return lna_bucket(self.cx.lna), (self.cx.pnp + 127) // 128
+
+    @property
     def device_bytes(self) -> int:
         return int(self.ctx._lib.gd_complex_device_bytes(self.h))
 
@@ -421,6 +426,24 @@ def run(cx: abi.Complex, steps_total: int, steps_per_exchange: int, minus_beta, 
     buf = abi.McLogBuffers(n_rep, len(mb), steps_total, bool(params.flags & abi.MC_RECORD))
     check(load().gd_run(C.byref(cx.struct()), C.byref(params), C.byref(buf.log)), "gd_run")
     return buf
+
+
+def lna_bucket(lna: int) -> int:
+    """Ligand-size bucket of the launch-shape cache (lna rounded up to 8)."""
+    return min(((lna + 7) // 8) * 8, 128)
+
+
+def autotune_buckets(dcxs):
+    """Autotunes one launch shape per size class of a batch: the largest
+    ligand of each (bucket, protein tiles) class is timed and its shape is
+    kept in the context for every ligand of the class.
+    Returns {size_class: ((A, P, NA), ms)}."""
+    rep = {}
+    for d in dcxs:
+        k = d.size_class
+        if k not in rep or d.cx.lna > rep[k].cx.lna:
+            rep[k] = d
+    return {k: d.autotune() for k, d in sorted(rep.items())}
 
 
 def fma_peak(ctx: Context, n_blocks: int = 148 * 16, iters: int = 4096):

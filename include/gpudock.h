@@ -238,12 +238,16 @@ typedef struct gd_tile {
   int atoms_per_warp;
 } gd_tile;
 
-/* Times every compiled launch shape for this complex's size class (ligand
- * atoms, protein tiles) on one wave of pose CTAs, keeps the fastest in the
- * context and returns it; later launches of that size class use it. */
+/* Times every compiled launch shape for this complex's size class on one
+ * wave of pose CTAs, keeps the fastest in the context and returns it; later
+ * launches of that size class use it.  A size class is (ligand-size bucket,
+ * protein tiles): ligand sizes are rounded up to a multiple of 8 atoms and a
+ * class's shape covers the bucket's largest size, so the ligands of a batch
+ * that fall in one bucket share one launch shape. */
 gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *dcx, gd_tile *best,
                       double *best_ms);
-/* Sets the launch shape of a size class explicitly. */
+/* Sets the launch shape of a size class explicitly (it must cover the
+ * bucket of lna, i.e. lna rounded up to a multiple of 8). */
 gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile);
 
 /* ------------------------------------------------------------------------ */
@@ -353,9 +357,12 @@ gd_status gd_remc_run(gd_remc *remc, int n_steps);
 gd_status gd_remc_read(gd_remc *remc, gd_mc_log *log);
 gd_status gd_remc_destroy(gd_remc *remc);
 int gd_remc_n_rep(const gd_remc *remc);
-/* Per-launch CUDA-event timing of the MC-interval and exchange kernels
- * issued by gd_remc_run while profiling is on; gd_remc_kernel_times
- * synchronises, returns the sums since the previous call and resets them. */
+/* CUDA-event timing of the MC kernels and exchange kernels issued by
+ * gd_remc_run / gd_batch_run while profiling is on.  One MC sample spans the
+ * launches of all launch shapes of one interval (they run side by side on
+ * side streams), so with a single shape it is one kernel's duration.
+ * gd_remc_kernel_times synchronises, returns the sums and sample counts
+ * since the previous call and resets them. */
 gd_status gd_remc_set_profiling(gd_remc *remc, int on);
 gd_status gd_remc_kernel_times(gd_remc *remc, double *mc_ms, int *mc_launches,
                                double *exch_ms, int *exch_launches);
