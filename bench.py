@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the plain / batched / served / pose-sweep measurements")
+    ap.add_argument("--tile", default=None,
+                    help="launch shape A,P,NA of the headline workload instead of the "
+                         "autotuner's (e.g. 4,3,10)")
     return ap.parse_args()
 
 
@@ -150,7 +153,7 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
     orc.mc_sample(cx, params, 0, threads, 1, threads, native)
     t1 = time.perf_counter() - t0
     per = max(t1, 1e-4)  # seconds for `threads` replica-steps
-    n_steps = max(1, min(50, int(budget_s / per / 4)))
+    n_steps = max(1, min(2000, int(budget_s / per / 4)))
     n_rep = min(n_rep_total, threads * 4)
     t0 = time.perf_counter()
     done = orc.mc_sample(cx, params, 0, n_rep, n_steps, threads, native)
@@ -239,6 +242,13 @@ def form_batched(ctx, stream, seed, flush, n_steps=50):
            "autotune_s": tune_s,
            "tiles": {f"lna<={k[0]},tiles={k[1]}": list(v[0]) for k, v in tuned.items()}}
     b.close()
+    # exchange-cadence autotuner on a one-wave subset of the ligands
+    cad, table = lib.autotune_cadence(ctx, dcxs[:148], mb, candidates=(1, 2, 5, 10, 20),
+                                      steps=40, move_scale=w.move_scale, seed=seed,
+                                      flags=abi.MC_EXCHANGE)
+    out["cadence"] = {"chosen_steps_per_exchange": cad,
+                      "ms_per_mc_step": {str(k): v for k, v in table.items()},
+                      "sample": "148 of the 512 ligands, 40 MC steps per candidate"}
     for d in dcxs:
         d.close()
     base.close()
@@ -401,7 +411,12 @@ def main():
     torch.cuda.set_stream(stream)
     ctx = lib.Context(local, stream.cuda_stream)
     dcx = lib.DeviceComplex(ctx, cx)
-    tile, _ = dcx.autotune()  # launch shape of this size class, kept in ctx
+    if args.tile:
+        tile = tuple(int(v) for v in args.tile.split(","))
+        lib.check(ctx._lib.gd_ctx_set_tile(ctx.h, cx.lna, cx.pnp, abi.GdTile(*tile)),
+                  "gd_ctx_set_tile")
+    else:
+        tile, _ = dcx.autotune()  # launch shape of this size class, kept in ctx
     total_steps = spe * (args.warmup + args.steps + 2)
     remc = lib.Remc(dcx, total_steps, spe, mb, w.move_scale, seed=args.seed + rank)
     remc.init()

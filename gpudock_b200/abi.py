@@ -21,6 +21,8 @@ TERM_NAMES = ("vdw", "ele", "pmf", "psp", "hdb", "hpc", "kde", "lhm", "dst", "to
 MC_EXCHANGE = 0x1
 MC_MOVE_AWAY = 0x2
 MC_RECORD = 0x4
+MC_MCC = 0x8
+CMCC_INVALID = 10000.0
 
 STATUS = {
     0: "GD_OK", 1: "GD_EINVAL", 2: "GD_ENOMEM", 3: "GD_EBUDGET", 4: "GD_ECUDA",

@@ -1,6 +1,6 @@
 // gd_api.cu -- host side of the C-ABI in include/gpudock.h: errors, force
 // field and temperature tables, validation, contexts, the device layout of a
-// complex, pose energies, the launch-shape autotuner and test entry points.
+// complex, pose energies, launch-shape selection and test entry points.
 //
 // Boundary replaced: the table staging of Run() in
 // gpudocksm-rem-1.2/src/run.cu:114-256 (cudaMemcpy / cudaMemcpyToSymbol into
@@ -43,23 +43,29 @@ int round_na(int na) {
   return 0;
 }
 
-// Default launch shape: about four atoms per warp (enough independent pair
-// chains to cover the MUFU and FMA latencies), atom groups to cover the
-// ligand, and when the protein is resident as many tile groups as fit in
-// MAX_WARPS.
+// Default launch shape (used until the autotuner has timed a size class):
+// atom groups to cover the ligand, and when the protein is resident as many
+// tile groups as fit in MAX_WARPS.
 Tile default_tile(int lna, bool resident) {
-  Tile t;
-  int na = lna <= 48 ? 4 : (lna <= 72 ? 6 : (lna <= 96 ? 8 : 10));
-  int A = (lna + na - 1) / na;
-  while (A > MAX_WARPS) {
-    na = round_na(na + 1);
-    A = (lna + na - 1) / na;
+  // A warp's time per protein point is about NA + 1.5 pair-slots (its atoms
+  // plus the per-point loads and test), and the A x P warps share the points
+  // P ways: pick the shape with the smallest (NA + 1.5) / P.
+  Tile best;
+  double best_cost = 1e30;
+  for (int na : kNAValues) {
+    const int A = (lna + na - 1) / na;
+    if (A > MAX_WARPS) continue;
+    const int NA = round_na((lna + A - 1) / A);
+    const int P = resident ? std::max(1, MAX_WARPS / A) : 1;
+    const double cost = (NA + 1.5) / P;
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best.A = A;
+      best.P = P;
+      best.NA = NA;
+    }
   }
-  na = round_na((lna + A - 1) / A);
-  t.A = A;
-  t.NA = na;
-  t.P = resident ? std::max(1, MAX_WARPS / A) : 1;
-  return t;
+  return best;
 }
 
 void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident) {
@@ -377,13 +383,19 @@ static gd_status upload_protein(const gd_protein &P, gd_dcomplex *d) {
   KTables &T = d->T;
   const int pnp = P.pnp;
   const int pnp_pad = (pnp + TILE_PTS - 1) / TILE_PTS * TILE_PTS;
-  std::vector<float4> pa((size_t)P.n_conf * pnp_pad, make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<float4> pa((size_t)P.n_conf * pnp_pad,
+                         make_float4(PAD_POINT_COORD, PAD_POINT_COORD, PAD_POINT_COORD, 0.f));
   for (int c = 0; c < P.n_conf; ++c)
     for (int p = 0; p < pnp; ++p) {
       const size_t i = (size_t)c * pnp + p;
       pa[(size_t)c * pnp_pad + p] = make_float4(P.x[i], P.y[i], P.z[i], P.ele[p]);
     }
-  std::vector<float2> pb((size_t)pnp_pad, make_float2(0.f, 0.f));
+  float pad_meta;
+  {
+    const uint32_t m = (uint32_t)PAD_POINT_TYPE;
+    std::memcpy(&pad_meta, &m, 4);
+  }
+  std::vector<float2> pb((size_t)pnp_pad, make_float2(0.f, pad_meta));
   for (int p = 0; p < pnp; ++p) {
     uint32_t meta = (uint32_t)P.t[p] | ((uint32_t)P.c[p] << META_CLASS_SHIFT) |
                     ((uint32_t)P.seq3r[p] << META_SEQ_SHIFT);
@@ -474,11 +486,27 @@ static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
   T.kde2 = F.kde2;
   T.kde3 = F.kde3;
   T.s2pi = sqrtf(2.0f * kPI);
-  // every close-range term fires inside this squared distance: hydrophobic
-  // d^2 <= 81, near-field electrostatics el1 d < 1, psp d <= pmf0
+  // the close-range terms fire inside these distances: near-field
+  // electrostatics el1 d < 1 (every point), hydrophobic d <= 9 (points with
+  // the hpc flag), psp d <= pmf0 (class-2 points); thresholds by point kind
+  // (hpc flag | class 2 << 1), squared with a margin for rounding
   const float r_ele = F.el1 > 0.f ? 1.0f / F.el1 : 1e30f;
-  const float r_max = std::max(9.0f, std::max(r_ele, max_pmf0));
-  T.near_d2 = r_max * r_max * 1.0001f + 1e-3f;
+  for (int kind = 0; kind < 4; ++kind) {
+    float r = r_ele;
+    if (kind & 1) r = std::max(r, 9.0f);
+    if (kind & 2) r = std::max(r, max_pmf0);
+    T.near4[kind] = r * r * 1.0001f + 1e-3f;
+  }
+  // kernel slot order: atoms with an H-bond term (some point type with
+  // hdb0 > 0.1) first, so that they share atom pairs and warps
+  std::vector<int> order;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int a = 0; a < lna; ++a) {
+      bool hb = false;
+      for (int j = 0; j < GD_NPT; ++j) hb = hb || F.hdb0[L.t[a]][j] > 0.1f;
+      if (hb == (pass == 0)) order.push_back(a);
+    }
+  GD_TRY(upload(d, order, &T.lig_order));
   for (int i = 0; i < GD_NLT; ++i) {
     T.hpl0[i] = F.hpl0[i];
     T.hpl1[i] = F.hpl1[i];
@@ -493,6 +521,46 @@ static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
     T.lig_center[i] = L.center[i];
     T.pocket[i] = cx->prt.pocket_center[i];
   }
+  return GD_OK;
+}
+
+// Reference contact map of the MCC score (InitRefMatrix_d,
+// calcmcc_d.cu:57-83): pairs with dst <= pmf0 for ligand conformation 0 in
+// its start pose (relative coordinates + centre, util.C:230-247) against the
+// complex's first protein conformation, in the reference's single-precision
+// order; one bit per (atom, point), rows of pnp_pad / 32 words.
+static gd_status upload_mcc_ref(const gd_complex *cx, int prt_conf, gd_dcomplex *d) {
+  const gd_ligand &L = cx->lig;
+  const gd_protein &P = cx->prt;
+  const gd_enepara &F = *cx->ff;
+  KTables &T = d->T;
+  const int words = T.pnp_pad / 32;
+  const int pc = prt_conf < P.n_conf ? prt_conf : 0;
+  std::vector<uint32_t> bits((size_t)L.lna * words, 0u);
+  int nref = 0;
+  float max_pmf0 = 0.f;
+  for (int i = 0; i < GD_NLT; ++i)
+    for (int j = 0; j < GD_NPT; ++j) max_pmf0 = std::max(max_pmf0, F.pmf0[i][j]);
+  for (int a = 0; a < L.lna; ++a) {
+    const float lx = L.x[a] + L.center[0];
+    const float ly = L.y[a] + L.center[1];
+    const float lz = L.z[a] + L.center[2];
+    for (int p = 0; p < P.pnp; ++p) {
+      const size_t i = (size_t)pc * P.pnp + p;
+      const float dx = lx - P.x[i];
+      const float dy = ly - P.y[i];
+      const float dz = lz - P.z[i];
+      const float dst = sqrtf(dx * dx + dy * dy + dz * dz);
+      if (dst <= F.pmf0[L.t[a]][P.t[p]]) {
+        bits[(size_t)a * words + (p >> 5)] |= 1u << (p & 31);
+        ++nref;
+      }
+    }
+  }
+  GD_TRY(upload(d, bits, &T.mcc_ref));
+  T.mcc_words = words;
+  T.mcc_nref = (float)nref;
+  T.near_mcc2 = max_pmf0 * max_pmf0 * 1.0001f + 1e-3f;
   return GD_OK;
 }
 
@@ -530,6 +598,7 @@ static gd_status complex_upload_common(gd_ctx *ctx, const gd_complex *cx,
       st = upload_protein(cx->prt, d);
     }
     if (st == GD_OK) st = upload_ligand(cx, d);
+    if (st == GD_OK) st = upload_mcc_ref(cx, share ? prt_conf0 : 0, d);
     if (st == GD_OK) {
       cudaError_t e = cudaStreamSynchronize(ctx->stream);
       if (e != cudaSuccess) st = fail(GD_ECUDA, "upload: %s", cudaGetErrorString(e));
@@ -647,85 +716,6 @@ extern "C" gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *d, int prt_
     return st;
   }
   return ctx_check(ctx);
-}
-
-// ---------------------------------------------------------------------------
-// Launch-shape autotuner: times the energy kernel on one wave of CTAs of
-// random poses for every compiled shape that covers the ligand and keeps the
-// fastest; the choice is cached in the context per (ligand atoms, protein
-// tiles) and used by every later launch for that size class.
-// ---------------------------------------------------------------------------
-extern "C" gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *d, gd_tile *best,
-                                 double *best_ms) {
-  if (!ctx || !d) return fail(GD_EINVAL, "gd_autotune: NULL handle");
-  GD_CUDA(cudaSetDevice(ctx->device));
-  const int lna = lna_bucket(d->T.lna);  // the tile must cover the whole size bucket
-  const int n_pose = 32 * ctx->n_sm;
-  std::vector<float> hp((size_t)n_pose * 6);
-  uint32_t s = 12345u;
-  for (auto &v : hp) {
-    s = s * 1664525u + 1013904223u;
-    v = ((s >> 8) * 0x1p-24f - 0.5f) * 2.0f;  // within +-1 A / +-1 rad
-  }
-  float *dp = nullptr, *dt = nullptr;
-  GD_CUDA(cudaMalloc(&dp, hp.size() * sizeof(float)));
-  GD_CUDA(cudaMalloc(&dt, (size_t)n_pose * GD_NTERM * sizeof(float)));
-  GD_CUDA(cudaMemcpy(dp, hp.data(), hp.size() * sizeof(float), cudaMemcpyHostToDevice));
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  Tile best_t;
-  float best_time = 1e30f;
-  gd_status st = GD_OK;
-  for (int na : kNAValues) {
-    const int A = (lna + na - 1) / na;
-    if (A > MAX_WARPS || (A > 1 && round_na((lna + A - 1) / A) != na)) continue;
-    for (int P = 1; A * P <= MAX_WARPS; ++P) {
-      Tile t;
-      t.A = A;
-      t.P = P;
-      t.NA = na;
-      if (A * P < 4 && A * P * 2 <= MAX_WARPS) continue;  // too few warps per SM
-      int ns, res;
-      pick_stages(d->T, t, &ns, &res);
-      if (!res && P > 1) continue;
-      float ms_min = 1e30f;
-      for (int rep = 0; rep < 3 && st == GD_OK; ++rep) {
-        KItem *dit = nullptr;
-        cudaEventRecord(e0, ctx->stream);
-        st = poses_launch(ctx, d, t, 0, 0, n_pose, dp, dt, nullptr, &dit);
-        cudaEventRecord(e1, ctx->stream);
-        cudaEventSynchronize(e1);
-        if (dit) cudaFree(dit);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (rep > 0) ms_min = std::min(ms_min, ms);
-      }
-      if (st != GD_OK) break;
-      if (ms_min < best_time) {
-        best_time = ms_min;
-        best_t = t;
-      }
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(dp);
-  cudaFree(dt);
-  GD_TRY(st);
-  GD_TRY(ctx_check(ctx));
-  if (!best_t.valid()) return fail(GD_EINVAL, "no launch shape fits lna=%d", lna);
-  {
-    std::lock_guard<std::mutex> g(ctx->tile_mu);
-    ctx->tiles[{lna, (d->T.pnp + TILE_PTS - 1) / TILE_PTS}] = best_t;
-  }
-  if (best) {
-    best->atom_groups = best_t.A;
-    best->tile_groups = best_t.P;
-    best->atoms_per_warp = best_t.NA;
-  }
-  if (best_ms) *best_ms = best_time;
-  return GD_OK;
 }
 
 extern "C" gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile) {

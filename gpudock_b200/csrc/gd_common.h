@@ -43,7 +43,8 @@ struct Tile {
 };
 
 // Candidate atoms-per-warp values compiled into the kernel.
-constexpr int kNAValues[] = {1, 2, 3, 4, 5, 6, 8, 10};
+// Even: the pair loop handles two atoms per packed f32x2 instruction.
+constexpr int kNAValues[] = {2, 4, 6, 8, 10};
 
 Tile default_tile(int lna, bool resident);
 int round_na(int na);  // smallest compiled NA >= na (0 if none)

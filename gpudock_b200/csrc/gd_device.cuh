@@ -153,7 +153,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
       : "memory");
 }
 
-// Barrier over the compute warps only (the producer warp never joins).
+// Orders shared-memory accesses made through the generic proxy (ordinary
+// loads of a staged tile) before later async-proxy writes (a bulk copy that
+// refills the same stage).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Named barrier over nthreads threads of the CTA.
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }

@@ -45,7 +45,7 @@ struct Ens {
   std::vector<KItem> items;
   KItem *d_items = nullptr;
   int n_rep_total = 0, spe = 0, step = 0;
-  float *m_old = nullptr, *e_old = nullptr, *minus_beta = nullptr;
+  float *m_old = nullptr, *e_old = nullptr, *minus_beta = nullptr, *cmcc = nullptr;
   int *idx_tmp = nullptr, *acs_mc = nullptr, *acs_exchg = nullptr, *d_step = nullptr;
   std::vector<Plan> plans;
   KGroup *d_groups = nullptr;
@@ -149,12 +149,14 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     I.seed = mc[i].seed;
     I.stream_id = mc[i].stream_id;
     I.flags = mc[i].flags;
+    I.spe = mc[i].steps_per_exchange;
     total += I.n_rep;
   }
   if (total > (1LL << 30)) return fail(GD_EINVAL, "too many replicas: %lld", total);
   E.n_rep_total = (int)total;
   GD_TRY(dalloc(E, &E.m_old, (size_t)total * 6));
   GD_TRY(dalloc(E, &E.e_old, (size_t)total * GD_NTERM));
+  GD_TRY(dalloc(E, &E.cmcc, (size_t)total));
   GD_TRY(dalloc(E, &E.idx_tmp, (size_t)total));
   GD_TRY(dalloc(E, &E.acs_mc, (size_t)total));
   GD_TRY(dalloc(E, &E.acs_exchg, (size_t)n * MAX_TMP));
@@ -171,6 +173,7 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     I.acs_exchg = E.acs_exchg + (size_t)i * MAX_TMP;
     I.m_old = E.m_old + (size_t)I.rep_base * 6;
     I.e_old = E.e_old + (size_t)I.rep_base * GD_NTERM;
+    I.cmcc = E.cmcc + I.rep_base;
     I.idx_tmp = E.idx_tmp + I.rep_base;
     I.acs_mc = E.acs_mc + I.rep_base;
     I.record = nullptr;
@@ -609,4 +612,129 @@ extern "C" gd_status gd_batch_kernel_times(gd_batch *b, double *mc_ms, int *mc_l
   if (!b || !mc_ms || !mc_launches || !exch_ms || !exch_launches)
     return fail(GD_EINVAL, "gd_batch_kernel_times: NULL argument");
   return ens_kernel_times(b->e, mc_ms, mc_launches, exch_ms, exch_launches);
+}
+
+// ---------------------------------------------------------------------------
+// Launch-shape autotuner.  Every compiled shape that covers the complex's
+// ligand-size bucket is timed on the REMC kernel itself: a temporary batch of
+// copies of the complex, 32 temperatures per exchange group (one group per
+// CTA, exchange inside the kernel), at least one CTA per SM, a few MC steps
+// per sample.  The fastest shape is cached in the context for the size class
+// (bucket, protein tiles) and used by every later launch of that class.
+// ---------------------------------------------------------------------------
+namespace {
+
+gd_status time_shape(gd_ctx *ctx, const gd_dcomplex *d, const std::vector<gd_mc_params> &mc,
+                     int n_items, int steps, float *ms) {
+  std::vector<const gd_dcomplex *> ds(n_items, d);
+  Ens E;
+  gd_status st = ens_build(E, ctx, n_items, ds.data(), mc.data());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == GD_OK) st = ens_init(E);
+  if (st == GD_OK) st = ens_run(E, steps);  // warm-up
+  if (st == GD_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    st = fail(GD_ECUDA, "autotune: event creation");
+  float best = 1e30f;
+  for (int rep = 0; rep < 2 && st == GD_OK; ++rep) {
+    cudaEventRecord(e0, ctx->stream);
+    st = ens_run(E, steps);
+    cudaEventRecord(e1, ctx->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(GD_ECUDA, "autotune: sync");
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    best = std::min(best, t);
+  }
+  if (st == GD_OK) st = ctx_check(ctx);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  ens_free(E);
+  *ms = best;
+  return st;
+}
+
+}  // namespace
+
+extern "C" gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *d, gd_tile *best,
+                                 double *best_ms) {
+  if (!ctx || !d) return fail(GD_EINVAL, "gd_autotune: NULL handle");
+  if (d->ctx != ctx) return fail(GD_EINVAL, "gd_autotune: complex belongs to another context");
+  GD_CUDA(cudaSetDevice(ctx->device));
+  const KTables &T = d->T;
+  const int hi = lna_bucket(T.lna);  // the shape must cover the whole bucket
+  const std::pair<int, int> key{hi, (T.pnp + TILE_PTS - 1) / TILE_PTS};
+  // 32 temperatures: one exchange group fills a CTA whatever the complex's
+  // conformation counts; enough copies for one CTA per SM
+  constexpr int kTmp = 32, kSpe = 2, kSteps = 4;
+  std::vector<float> mb(kTmp);
+  for (int t = 0; t < kTmp; ++t) mb[t] = -1.0f / (0.004f * powf(10.0f, t / (float)(kTmp - 1)));
+  const int groups = T.n_prt * T.n_lig;
+  const int n_items = std::max(1, std::min(256, (ctx->n_sm + groups - 1) / groups));
+  gd_mc_params p{};
+  p.steps_total = 1 << 20;
+  p.steps_per_exchange = kSpe;
+  p.steps_per_dump = 0;
+  p.n_tmp = kTmp;
+  for (int i = 0; i < 6; ++i) p.move_scale[i] = i < 3 ? 0.02f : 0.08f;
+  p.minus_beta = mb.data();
+  p.seed = 12345;
+  p.flags = GD_MC_EXCHANGE;
+  std::vector<gd_mc_params> mc(n_items, p);
+  for (int i = 0; i < n_items; ++i) mc[i].stream_id = (uint32_t)i;
+
+  bool had = false;
+  Tile prev;
+  {
+    std::lock_guard<std::mutex> g(ctx->tile_mu);
+    auto it = ctx->tiles.find(key);
+    if (it != ctx->tiles.end()) {
+      had = true;
+      prev = it->second;
+    }
+  }
+  Tile best_t;
+  float best_time = 1e30f;
+  gd_status st = GD_OK;
+  for (int na : kNAValues) {
+    const int A = (hi + na - 1) / na;
+    if (A > MAX_WARPS || (A > 1 && round_na((hi + A - 1) / A) != na)) continue;
+    for (int P = 1; A * P <= MAX_WARPS && st == GD_OK; ++P) {
+      Tile t;
+      t.A = A;
+      t.P = P;
+      t.NA = na;
+      if (A * P < 4 && A * P * 2 <= MAX_WARPS) continue;  // too few warps per SM
+      int ns, res;
+      pick_stages(T, t, &ns, &res);
+      if (!res && P > 1) continue;
+      {
+        std::lock_guard<std::mutex> g(ctx->tile_mu);
+        ctx->tiles[key] = t;
+      }
+      float ms = 1e30f;
+      st = time_shape(ctx, d, mc, n_items, kSteps, &ms);
+      if (st == GD_OK && ms < best_time) {
+        best_time = ms;
+        best_t = t;
+      }
+    }
+    if (st != GD_OK) break;
+  }
+  {
+    std::lock_guard<std::mutex> g(ctx->tile_mu);
+    if (st == GD_OK && best_t.valid())
+      ctx->tiles[key] = best_t;
+    else if (had)
+      ctx->tiles[key] = prev;
+    else
+      ctx->tiles.erase(key);
+  }
+  GD_TRY(st);
+  if (!best_t.valid()) return fail(GD_EINVAL, "no launch shape fits lna=%d", T.lna);
+  if (best) {
+    best->atom_groups = best_t.A;
+    best->tile_groups = best_t.P;
+    best->atoms_per_warp = best_t.NA;
+  }
+  if (best_ms) *best_ms = best_time;
+  return GD_OK;
 }

@@ -14,10 +14,13 @@ namespace gd {
 constexpr int TILE_PTS = 128;
 constexpr int STREAM_STAGES = 8;       // ring depth when the protein streams
 constexpr int MAX_RESIDENT_TILES = 56; // 7168 points kept in smem for a launch
-constexpr int MAX_WARPS = 12;          // compute warps per CTA (plus 1 producer)
+#ifndef GD_MAX_WARPS
+#define GD_MAX_WARPS 12
+#endif
+constexpr int MAX_WARPS = GD_MAX_WARPS; // warps per CTA (all compute)
 constexpr int MAX_NA = 10;             // ligand atoms per warp (template bound)
 constexpr int MAX_LNA = 128;           // ligand atoms per complex
-constexpr int NRED = 8;                // partial sums per replica per warp
+constexpr int NRED = 10;               // partial sums per replica per warp
 constexpr int MAX_TMP = 64;            // temperatures per exchange group
 constexpr int TAB_ROWS = GD_NLT + 1;   // + one all-zero row for padding atoms
 
@@ -28,6 +31,12 @@ constexpr uint32_t META_CLASS_SHIFT = 5u;
 constexpr uint32_t META_HPC_BIT = 1u << 8;
 constexpr uint32_t META_SEQ_SHIFT = 12u;
 constexpr int MAX_SEQ3R = (1 << 20) - 1;
+// Points past the protein's last point (up to the tile boundary) are padding:
+// type PAD_POINT_TYPE, whose kernel table rows are all zero, no charge, and
+// far from everything (on the opposite side from the padding ligand atoms),
+// so the pair loop may run over them and add exactly zero.
+constexpr int PAD_POINT_TYPE = 31;
+constexpr float PAD_POINT_COORD = -1.0e4f;
 
 enum KMode : int { KMODE_POSES = 0, KMODE_REMC = 1, KMODE_INIT = 2 };
 
@@ -38,6 +47,8 @@ struct KTables {
   const float4 *tab_a;  // [TAB_ROWS*NPT] {p1a, p2a, pmf0, pmf1}
   const float2 *tab_b;  // [TAB_ROWS*NPT] {hdb0, hdb1}
   const float4 *lig;    // [n_lig][lna] {x, y, z, 0} relative to the centre
+  const int *lig_order; // [lna] atom of each kernel slot: atoms with an H-bond
+                        // term first, so they share atom pairs and warps
   const int *lig_t;     // [lna]
   const float *lig_q;   // [lna]
   const float *psp;     // [NLT][psp_ncol]
@@ -46,10 +57,14 @@ struct KTables {
   const float4 *mcs;    // [pos][lna] {x, y, z, valid}
   const float *mcs_tcc; // [pos]
   const float *mcs_cnt; // [pos] number of valid atoms (float)
-  int lna, n_lig, pnp, pnp_pad, n_prt, pos, psp_ncol, pad0;
+  const uint32_t *mcc_ref;  // [lna][mcc_words] reference contact map (bits)
+  int lna, n_lig, pnp, pnp_pad, n_prt, pos, psp_ncol, mcc_words;
+  float mcc_nref;       // contacts in the reference map
+  float near_mcc2;      // squared distance within which a contact can occur
   float lj0, lj0lj1, el0, el1, inv_el1, a1, b1, kde2, kde3;
   float s2pi;           // sqrtf(2 * 3.1415926535f), the reference's float
-  float near_d2;        // squared distance below which a rare term can fire
+  float near4[4];       // squared distance below which a close-range term can
+                        // fire, by point kind (hpc flag | class 2 << 1)
   float hpl0[GD_NLT], hpl1[GD_NLT], hpl2[GD_NLT];
   float a_para[GD_NTERM], b_para[GD_NTERM], w[GD_NTERM];
   float lig_center[3], pocket[3];
@@ -64,6 +79,8 @@ struct KItem {
   int steps_per_dump;    // exchange parity restarts every dump (<= 0: never)
   int rec_steps;
   int step0;             // first MC step of the launch when KRun.item_step
+  int n_run;             // MC steps of the launch when KRun.item_step
+  int spe;               // steps per exchange (exchange kernel, per-item mode)
   float move_scale[6];
   uint64_t seed;
   uint32_t stream_id, flags;
@@ -73,6 +90,7 @@ struct KItem {
   // replica state of this item, indexed by its local replica number
   float *m_old;             // [n_rep][6]
   float *e_old;             // [n_rep][GD_NTERM]
+  float *cmcc;              // [n_rep] contact MCC of the state (GD_MC_MCC)
   int *idx_tmp;             // [n_rep]
   int *acs_mc;              // [n_rep]
 };
@@ -98,9 +116,9 @@ struct KRun {
   const float *poses;    // [n_pose][6]
   float *terms;          // [n_pose][GD_NTERM]
   double *raw;           // [n_pose][GD_NRAW] or nullptr
-  // REMC: the first MC step is KItem.step0 with item_step (complexes at
-  // different steps in one launch), else *step_ptr when step_ptr is set
-  // (graph replay), else step0
+  // REMC: the first MC step and the step count are KItem.step0 / n_run with
+  // item_step (complexes at different steps in one launch), else the first
+  // step is *step_ptr when step_ptr is set (graph replay), else step0
   int step0, n_steps;
   const int *step_ptr;
   int item_step;

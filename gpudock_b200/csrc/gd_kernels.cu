@@ -7,8 +7,9 @@
 // ligand atoms a = ag + A k in registers and sweeps the protein tiles
 // t = pg, pg + P, ...  The protein conformation is staged in shared memory in
 // 128-point tiles by the TMA engine (cp.async.bulk + mbarrier), once per
-// launch when it fits (resident) or through an 8-stage ring fed by a
-// producer warp (then P = 1).  Per step every warp writes FP64 partial sums
+// launch when it fits (resident) or through an 8-stage ring that the last
+// warp to finish a stage refills (then P = 1).  Per step every warp writes
+// FP64 partial sums
 // per replica; warp 0 reduces them in a fixed order, normalises the terms
 // and takes the Metropolis decision with the counter-based RNG.
 //
@@ -38,12 +39,22 @@
 
 namespace gd {
 
-constexpr int TAB_N = TAB_ROWS * GD_NPT;
-constexpr int TAB_BYTES = TAB_N * (16 + 8);
 constexpr int STAGE_BYTES = TILE_PTS * (16 + 8);
 constexpr int CHUNK = 32;  // points per FP32 partial before the FP64 flush
 constexpr float LOG2E = 1.4426950408889634f;
 constexpr float FAR = 1.0e4f;  // coordinate of the padding atoms
+// Point types of the kernel's pair tables: the force field's GD_NPT plus
+// all-zero rows, one of which (PAD_POINT_TYPE) marks the padding points that
+// fill a tile past the protein's last point, so they add exactly zero.
+constexpr int PT_ROWS = 32;
+// Largest atoms-per-warp count whose pair loop takes two protein points per
+// iteration (more independent work per warp); above it the registers do not
+// allow the second point.
+#ifndef GD_PTS2_MAX_NA
+#define GD_PTS2_MAX_NA 4
+#endif
+constexpr int PTS2_MAX_NA = GD_PTS2_MAX_NA;
+static_assert(PAD_POINT_TYPE >= GD_NPT && PAD_POINT_TYPE < PT_ROWS, "padding type row");
 
 // Per-replica state in shared memory, written by warp 0 only.
 struct LaneState {
@@ -55,17 +66,64 @@ struct LaneState {
   int idx_tmp;       // its temperature index
   int acs;           // accepted moves in this launch
   uint32_t u_bits;   // random word of this step's Metropolis test
+  float cmcc_old;    // contact MCC of the accepted state (GD_MC_MCC)
+  float cmcc_new;    // and of the proposal
   float pad;
 };
-static_assert(sizeof(LaneState) == 144, "LaneState layout");
+static_assert(sizeof(LaneState) == 152, "LaneState layout");
 static_assert(sizeof(KItem) % 8 == 0, "KItem must keep the barriers 8-byte aligned");
-static_assert(TAB_BYTES % 16 == 0, "tile staging must start 16-byte aligned");
+
+// Shared-memory carve-up of one CTA.  The pair tables hold, for every
+// (atom group, atom pair h, point type), the parameters of the warp's two
+// atoms of pair h side by side, so one 16-byte load yields the operand pairs
+// of the packed (f32x2) arithmetic:
+//   ptab[.][0] = {p1a a, p1a b, -p2a a, -p2a b}
+//   ptab[.][1] = {-pmf0 a, -pmf0 b, pmf1 a, pmf1 b}
+//   htab[.]    = {-hdb0 a, -hdb0 b, w a, w b}  (w = hdb1 where the H-bond
+//                                               term is defined, else 0)
+// hmask[ag][pt] has bit h set when pair h of group ag has an H-bond term with
+// point type pt.  Slot s = ag + A k holds ligand atom order[s].
+struct SmemLayout {
+  size_t ptab, htab, hmask, slot_q, slot_t, slot_a, tiles, red, hpc, lane, item, bars, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int A, int P, int NA, int NS) {
+  SmemLayout L;
+  const size_t NH = NA / 2, MAXA = (size_t)A * NA, W = (size_t)A * P;
+  size_t o = 0;
+  L.ptab = o;
+  o += (size_t)A * NH * PT_ROWS * 32;
+  L.htab = o;
+  o += (size_t)A * NH * PT_ROWS * 16;
+  L.hmask = o;
+  o += (size_t)A * PT_ROWS * 4;
+  L.slot_q = o;
+  o += MAXA * 4;
+  L.slot_t = o;
+  o += MAXA * 4;
+  L.slot_a = o;
+  o += MAXA * 4;
+  o = (o + 127) & ~size_t(127);
+  L.tiles = o;
+  o += (size_t)NS * STAGE_BYTES;
+  L.red = o;
+  o += W * NRED * 32 * sizeof(double);
+  L.hpc = o;
+  o += (size_t)P * MAXA * 32 * sizeof(float);
+  L.lane = o;
+  o += 32 * sizeof(LaneState);
+  o = (o + 15) & ~size_t(15);
+  L.item = o;
+  o += sizeof(KItem);
+  o = (o + 7) & ~size_t(7);
+  L.bars = o;
+  o += 2 * (size_t)NS * sizeof(uint64_t);
+  L.total = o;
+  return L;
+}
 
 size_t dock_smem_bytes(int A, int P, int NA, int n_stages) {
-  const int W = A * P;
-  return (size_t)TAB_BYTES + (size_t)n_stages * STAGE_BYTES +
-         (size_t)W * NRED * 32 * sizeof(double) + (size_t)P * A * NA * 32 * sizeof(float) +
-         32 * sizeof(LaneState) + sizeof(KItem) + (size_t)2 * n_stages * sizeof(uint64_t);
+  return smem_layout(A, P, NA, n_stages).total;
 }
 
 // Hardware approximations (PTX rsqrt / rcp / ex2, flush-to-zero).
@@ -84,6 +142,14 @@ __device__ __forceinline__ float fex2(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+
+// Packed FP32 pairs (Blackwell f32x2 FMA-pipe instructions).
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
 // Hydrophobic contact polynomial of calcenergy_d.cu:80-86 in Horner form:
 // 1 - (3.5/81 d2 - 4.5/81^2 d4 + 2.5/81^3 d6 - 0.5/81^4 d8)
@@ -121,9 +187,9 @@ __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R)
 // pair loop.
 template <int MODE>
 __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneState &me,
-                                         double *s_red, const float *s_hpc, int W, int P,
-                                         int MAXA, int lane, int rep, bool active, int prt_conf,
-                                         int lig_conf, int step) {
+                                         double *s_red, const float *s_hpc, const int *s_lt,
+                                         int W, int P, int MAXA, int lane, int rep, bool active,
+                                         int prt_conf, int lig_conf, int step) {
   const KTables &T = I.T;
   const int lna = T.lna;
   const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
@@ -135,11 +201,12 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
 #pragma unroll
       for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
     }
-    // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149)
+    // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149), by
+    // slot (slot a holds one atom, s_lt its type)
     for (int a = 0; a < lna; ++a) {
       float h = 0.f;
       for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
-      const int lt = T.lig_t[a];
+      const int lt = s_lt[a];
       const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
       S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
     }
@@ -172,6 +239,21 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
 #pragma unroll
     for (int i = 1; i < 9; ++i) tot = __fadd_rn(tot, __fmul_rn(T.w[i], e[i]));
     e[9] = tot;
+    if (MODE != KMODE_POSES && (I.flags & GD_MC_MCC)) {
+      // confusion counts against the reference map (calcmcc_d.cu:189-206);
+      // the counts are exact integers in FP32 below 2^24 pairs
+      const float tp = (float)S[9];
+      const float fp = __fsub_rn((float)S[8], tp);
+      const float fn = __fsub_rn(T.mcc_nref, tp);
+      const float n = __fmul_rn((float)T.lna, (float)T.pnp);
+      const float tn = __fsub_rn(__fsub_rn(__fsub_rn(n, tp), fn), fp);
+      const float dividend = __fsqrt_rn(
+          __fmul_rn(__fmul_rn(__fmul_rn(__fadd_rn(tp, fp), __fadd_rn(tp, fn)), __fadd_rn(tn, fp)),
+                    __fadd_rn(tn, fn)));
+      me.cmcc_new = dividend != 0.0f
+                        ? __fdiv_rn(__fsub_rn(__fmul_rn(tp, tn), __fmul_rn(fp, fn)), dividend)
+                        : GD_CMCC_INVALID;
+    }
 
     if (MODE == KMODE_POSES) {
       if (active) {
@@ -196,7 +278,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
           rc->idx_lig = lig_conf;
 #pragma unroll
           for (int i = 0; i < GD_NTERM; ++i) rc->e[i] = me.e_old[i];
-          rc->cmcc = 0.f;
+          rc->cmcc = (I.flags & GD_MC_MCC) ? me.cmcc_old : 0.f;
 #pragma unroll
           for (int i = 0; i < 6; ++i) rc->movematrix[i] = me.m_old[i];
           rc->step = step;
@@ -210,6 +292,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
         for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = e[i];
 #pragma unroll
         for (int i = 0; i < 6; ++i) me.m_old[i] = me.m_new[i];
+        me.cmcc_old = me.cmcc_new;
       }
       // temperature exchange of the CTA's own groups at the end of every
       // interval (exchangereplicas_d.cu:26-79); slot t of group gi is lane
@@ -259,43 +342,217 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
     }
   }
 
+struct PairConst {
+  float2 one, lj1, lj0, ca, cb;
+};
+
+// Terms of one atom pair (h) of this lane against one protein point (Ap),
+// two atoms per packed instruction: soft LJ, far-field electrostatics
+// (per-atom sums of ele/d), contact PMF and, with HDB, the H-bond term.  The
+// LJ and PMF quotients share one reciprocal: with D1 = p4 and
+// D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the point
+// type's entry of atom pair 0 of this warp's pair tables.
+template <bool HDB>
+__device__ __forceinline__ void pair_hh(float2 nx, float2 ny, float2 nz, const float4 &Ap,
+                                        const float4 *pp, const float4 *hp, int h,
+                                        const PairConst &K, float2 &fvdw, float2 &fpmf,
+                                        float2 &fhdb, float2 &fek, float &mn) {
+  const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
+  const float4 T1 = pp[h * 2 * PT_ROWS + 1];  // -pmf0, pmf1
+  const float2 dx = add2(dup2(Ap.x), nx);
+  const float2 dy = add2(dup2(Ap.y), ny);
+  const float2 dz = add2(dup2(Ap.z), nz);
+  const float2 d2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+  const float2 r = make_float2(frsqrt(d2.x), frsqrt(d2.y));
+  const float2 d = mul2(d2, r);
+  const float2 r2 = mul2(r, r);
+  const float2 r3 = mul2(r2, r);
+  const float2 r6 = mul2(r3, r3);
+  const float2 r9 = mul2(r6, r3);
+  const float2 p1 = mul2(lo2(T0), r9);
+  const float2 p12 = fma2(hi2(T0), r6, p1);  // p1 - p2
+  const float2 p4 = fma2(p1, fma2(K.lj1, d2, K.lj0), K.one);
+  const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
+  const float2 ex = make_float2(fex2(arg.x), fex2(arg.y));
+  const float2 e1 = add2(ex, K.one);
+  const float2 den = mul2(p4, e1);
+  const float2 inv = make_float2(frcp(den.x), frcp(den.y));
+  fvdw = fma2(mul2(p12, e1), inv, fvdw);
+  fpmf = fma2(mul2(hi2(T1), p4), inv, fpmf);
+  fek = fma2(dup2(Ap.w), r, fek);
+  mn = fminf(mn, fminf(d2.x, d2.y));
+  if (HDB) {
+    // weight 0 (and h3 = 0) for the atoms of the pair without the term
+    const float4 H = hp[h * PT_ROWS];  // -hdb0, w
+    const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
+    const float2 ha = mul2(mul2(h3, h3), K.ca);  // -0.5 log2(e) h3^2
+    fhdb = fma2(hi2(H), make_float2(fex2(ha.x), fex2(ha.y)), fhdb);
+  }
+}
+
+// One protein point against this lane's NA atoms (branch-free body).
+template <int NH, bool HDB>
+__device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2 (&ny)[NH],
+                                            const float2 (&nz)[NH], const float4 &A0,
+                                            const float4 *pp, const float4 *hp,
+                                            const PairConst &K, float2 &fvdw, float2 &fpmf,
+                                            float2 &fhdb, float2 (&fek)[NH], float &mn) {
+#pragma unroll
+  for (int h = 0; h < NH; ++h)
+    pair_hh<HDB>(nx[h], ny[h], nz[h], A0, pp, hp, h, K, fvdw, fpmf, fhdb, fek[h], mn);
+}
+
+// Two protein points (A0, A1) against this lane's NA atoms.  The body has no
+// branches, so the compiler interleaves the 2 x NA/2 independent chains; the
+// sums keep the order point A0 before A1 for every atom pair.
+template <int NH, bool HDB0, bool HDB1>
+__device__ __forceinline__ void pair_block2(const float2 (&nx)[NH], const float2 (&ny)[NH],
+                                            const float2 (&nz)[NH], const float4 &A0,
+                                            const float4 &A1, const float4 *pp0,
+                                            const float4 *pp1, const float4 *hp0,
+                                            const float4 *hp1, const PairConst &K, float2 &fvdw,
+                                            float2 &fpmf, float2 &fhdb, float2 (&fek)[NH],
+                                            float &mn0, float &mn1) {
+#pragma unroll
+  for (int h = 0; h < NH; ++h) {
+    pair_hh<HDB0>(nx[h], ny[h], nz[h], A0, pp0, hp0, h, K, fvdw, fpmf, fhdb, fek[h], mn0);
+    pair_hh<HDB1>(nx[h], ny[h], nz[h], A1, pp1, hp1, h, K, fvdw, fpmf, fhdb, fek[h], mn1);
+  }
+}
+
+// Close-range terms of one protein point (calcenergy_d.cu:80-138): the
+// hydrophobic contact per atom (points with the hpc flag, d <= 9 A), the
+// near-field electrostatics (el1 d < 1) and the pocket-specific potential
+// (class-2 points, d <= pmf0); with the MCC score on, the contacts d <= pmf0
+// of every point, counted (with those also in the reference map,
+// calcmcc_d.cu:148-213) straight into the lane's FP64 slots 8 and 9 of
+// my_red, so the rare counts hold no registers in the pair loop.  Distances
+// are recomputed per atom; p is the point's index in the protein.
+template <int NA>
+__device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const float2 (&ny)[NA / 2],
+                                            const float2 (&nz)[NA / 2], const float4 &Ap,
+                                            float hpp, uint32_t meta, const float4 *pp,
+                                            const KTables &T, const float *s_q, const int *s_lt,
+                                            const int *s_atom, float *my_hpc, int A, int ag,
+                                            int n_my, float inv_el1, float &fnear, float &fpsp,
+                                            bool mcc_on, int p, double *my_red) {
+  const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
+  const bool hflag = (meta & META_HPC_BIT) != 0u;
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    const float2 ax = nx[k >> 1], ay = ny[k >> 1], az = nz[k >> 1];
+    const float dx = (k & 1) ? ax.y + Ap.x : ax.x + Ap.x;
+    const float dy = (k & 1) ? ay.y + Ap.y : ay.x + Ap.y;
+    const float dz = (k & 1) ? az.y + Ap.z : az.x + Ap.z;
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (hflag && d2 <= 81.0f && k < n_my) {
+      float *hh = my_hpc + (size_t)A * k * 32;
+      *hh = fmaf(hpp, hpc_poly(d2), *hh);
+    }
+    const float rk = frsqrt(d2);
+    const float d = d2 * rk;
+    const float s1 = T.el1 * d;
+    if (s1 < 1.0f) {
+      const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
+      fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
+    }
+    if ((is_c2 || mcc_on) && k < n_my) {
+      const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
+      const float dm = d + ((k & 1) ? T1.y : T1.x);
+      if (dm <= 0.0f) {
+        if (is_c2)
+          fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + (meta >> META_SEQ_SHIFT)]);
+        if (mcc_on) {
+          const int a = s_atom[ag + A * k];
+          my_red[8 * 32] += 1.0;
+          if ((__ldg(&T.mcc_ref[(size_t)a * T.mcc_words + (p >> 5)]) >> (p & 31)) & 1u)
+            my_red[9 * 32] += 1.0;
+        }
+      }
+    }
+  }
+}
+
 template <int MODE, int NA>
-__global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
+// No producer warp: sm_100 splits the register file between the four
+// schedulers, so a 13th warp would put four warps on one scheduler and cap
+// every thread at 128 registers; 12 warps leave room for about 168.
+__global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     dock_kernel(const __grid_constant__ KRun R) {
+  static_assert(NA % 2 == 0, "atoms are processed in pairs");
+  constexpr int NH = NA / 2;
+  // protein points per loop iteration: two while the registers allow
+  constexpr int PTS = NA <= PTS2_MAX_NA ? 2 : 1;
   extern __shared__ __align__(128) unsigned char smem[];
   const int A = R.A, P = R.P, W = A * P, NS = R.n_stages;
   const int MAXA = A * NA;
-  float4 *s_tab_a = reinterpret_cast<float4 *>(smem);
-  float2 *s_tab_b = reinterpret_cast<float2 *>(smem + TAB_N * 16);
-  unsigned char *s_tiles = smem + TAB_BYTES;
-  double *s_red = reinterpret_cast<double *>(s_tiles + (size_t)NS * STAGE_BYTES);
-  float *s_hpc = reinterpret_cast<float *>(s_red + (size_t)W * NRED * 32);
-  LaneState *s_lane = reinterpret_cast<LaneState *>(s_hpc + (size_t)P * MAXA * 32);
-  KItem *s_item = reinterpret_cast<KItem *>(s_lane + 32);
-  uint64_t *s_full = reinterpret_cast<uint64_t *>(s_item + 1);
-  uint64_t *s_empty = s_full + NS;
+  const SmemLayout SL = smem_layout(A, P, NA, NS);
+  float4 *s_ptab = reinterpret_cast<float4 *>(smem + SL.ptab);
+  float4 *s_htab = reinterpret_cast<float4 *>(smem + SL.htab);
+  uint32_t *s_hmask = reinterpret_cast<uint32_t *>(smem + SL.hmask);
+  float *s_q = reinterpret_cast<float *>(smem + SL.slot_q);
+  int *s_lt = reinterpret_cast<int *>(smem + SL.slot_t);
+  int *s_atom = reinterpret_cast<int *>(smem + SL.slot_a);
+  unsigned char *s_tiles = smem + SL.tiles;
+  double *s_red = reinterpret_cast<double *>(smem + SL.red);
+  float *s_hpc = reinterpret_cast<float *>(smem + SL.hpc);
+  LaneState *s_lane = reinterpret_cast<LaneState *>(smem + SL.lane);
+  KItem *s_item = reinterpret_cast<KItem *>(smem + SL.item);
+  uint64_t *s_full = reinterpret_cast<uint64_t *>(smem + SL.bars);
+  int *s_done = reinterpret_cast<int *>(s_full + NS);  // warps done with a stage
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
 
-  // ---- item of this CTA into shared memory, type table, barriers ----------
+  // ---- item of this CTA into shared memory, pair tables, barriers ---------
   const int item = (MODE == KMODE_POSES) ? 0 : R.cta_item[blockIdx.x];
   const KItem &G = R.items[item];
   {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(&G);
     uint32_t *dst = reinterpret_cast<uint32_t *>(s_item);
     for (int i = threadIdx.x; i < (int)(sizeof(KItem) / 4); i += blockDim.x) dst[i] = src[i];
-    const float4 *ta = G.T.tab_a;
-    const float2 *tb = G.T.tab_b;
-    for (int i = threadIdx.x; i < TAB_N; i += blockDim.x) {
-      s_tab_a[i] = ta[i];
-      s_tab_b[i] = tb[i];
+    const KTables &TG = G.T;
+    const int lna = TG.lna;
+    // slot s holds atom order[s]; slots past the ligand are padding atoms
+    // (all-zero table row, no charge, far from everything)
+    for (int s = threadIdx.x; s < MAXA; s += blockDim.x) {
+      const int a = s < lna ? TG.lig_order[s] : -1;
+      s_atom[s] = a;
+      s_lt[s] = a >= 0 ? TG.lig_t[a] : GD_NLT;
+      s_q[s] = a >= 0 ? TG.lig_q[a] : 0.f;
+    }
+    // point types GD_NPT..PT_ROWS-1 (the padding points) get all-zero entries
+    for (int i = threadIdx.x; i < A * NH * PT_ROWS; i += blockDim.x) {
+      const int pt = i % PT_ROWS, h = (i / PT_ROWS) % NH, ag = i / (PT_ROWS * NH);
+      const int s0 = ag + A * (2 * h), s1 = s0 + A;
+      const int ptc = pt < GD_NPT ? pt : 0;
+      const int r0 = (s0 < lna && pt < GD_NPT ? TG.lig_t[TG.lig_order[s0]] : GD_NLT) * GD_NPT + ptc;
+      const int r1 = (s1 < lna && pt < GD_NPT ? TG.lig_t[TG.lig_order[s1]] : GD_NLT) * GD_NPT + ptc;
+      const float4 a0 = TG.tab_a[r0], a1 = TG.tab_a[r1];
+      s_ptab[2 * i] = make_float4(a0.x, a1.x, -a0.y, -a1.y);
+      s_ptab[2 * i + 1] = make_float4(-a0.z, -a1.z, a0.w, a1.w);
+      // H-bond term where hdb0 > 0.1 (calcenergy_d.cu:115-126)
+      const float2 b0 = TG.tab_b[r0], b1 = TG.tab_b[r1];
+      const bool h0 = b0.x > 0.1f, h1 = b1.x > 0.1f;
+      s_htab[i] = make_float4(h0 ? -b0.x : 0.f, h1 ? -b1.x : 0.f, h0 ? b0.y : 0.f,
+                              h1 ? b1.y : 0.f);
+    }
+    for (int i = threadIdx.x; i < A * PT_ROWS; i += blockDim.x) {
+      const int pt = i % PT_ROWS, ag = i / PT_ROWS;
+      uint32_t m = 0;
+      for (int h = 0; h < NH && pt < GD_NPT; ++h) {
+        const int s0 = ag + A * (2 * h), s1 = s0 + A;
+        const int r0 = (s0 < lna ? TG.lig_t[TG.lig_order[s0]] : GD_NLT) * GD_NPT + pt;
+        const int r1 = (s1 < lna ? TG.lig_t[TG.lig_order[s1]] : GD_NLT) * GD_NPT + pt;
+        if (TG.tab_b[r0].x > 0.1f || TG.tab_b[r1].x > 0.1f) m |= 1u << h;
+      }
+      s_hmask[i] = m;
     }
   }
   if (threadIdx.x == 0) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(&s_full[i], 1);
-      mbar_init(&s_empty[i], W);
+      s_done[i] = 0;
     }
     fence_barrier_init();
   }
@@ -327,34 +584,28 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   }
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
   const bool resident = R.resident != 0;
-  const int n_steps = (MODE == KMODE_REMC) ? R.n_steps : 1;
+  const int n_steps = (MODE != KMODE_REMC) ? 1 : (R.item_step ? I.n_run : R.n_steps);
   const int passes = resident ? 1 : n_steps;
   const int step_base = (MODE == KMODE_REMC && R.item_step)  ? I.step0
                         : (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr
                                                              : R.step0;
 
-  // ---- producer warp: stages the protein conformation -------------------
-  if (warp == W) {
-    if (lane == 0) {
-      const float4 *src_a = T.pt_a + (size_t)prt_conf * T.pnp_pad;
-      const float2 *src_b = T.pt_b;
-      int it = 0;
-      for (int pass = 0; pass < passes; ++pass) {
-        for (int t = 0; t < n_tiles; ++t, ++it) {
-          const int s = resident ? t : (it % NS);
-          if (!resident) {
-            const uint32_t ph = (uint32_t)((it / NS) & 1);
-            mbar_wait(&s_empty[s], ph ^ 1u, R.err, 1);
-          }
-          unsigned char *dst = s_tiles + (size_t)s * STAGE_BYTES;
-          mbar_arrive_expect_tx(&s_full[s], STAGE_BYTES);
-          bulk_g2s(dst, src_a + (size_t)t * TILE_PTS, TILE_PTS * 16, &s_full[s]);
-          bulk_g2s(dst + TILE_PTS * 16, src_b + (size_t)t * TILE_PTS, TILE_PTS * 8, &s_full[s]);
-        }
-      }
-    }
-    return;
-  }
+  // ---- protein staging: the tile sequence of the launch (every tile once
+  // when resident, else all tiles once per MC step through the NS-stage
+  // ring).  Thread 0 issues the first NS copies; afterwards the last warp to
+  // finish a stage (elected by the s_done counter) refills it.
+  const float4 *src_a = T.pt_a + (size_t)prt_conf * T.pnp_pad;
+  const float2 *src_b = T.pt_b;
+  const int n_seq = passes * n_tiles;
+  auto issue_tile = [&](int q) {
+    const int s = q % NS, t = q % n_tiles;
+    unsigned char *dst = s_tiles + (size_t)s * STAGE_BYTES;
+    mbar_arrive_expect_tx(&s_full[s], STAGE_BYTES);
+    bulk_g2s(dst, src_a + (size_t)t * TILE_PTS, TILE_PTS * 16, &s_full[s]);
+    bulk_g2s(dst + TILE_PTS * 16, src_b + (size_t)t * TILE_PTS, TILE_PTS * 8, &s_full[s]);
+  };
+  if (threadIdx.x == 0)
+    for (int q = 0; q < min(NS, n_seq); ++q) issue_tile(q);
 
   // ---- compute warps -----------------------------------------------------
   const int ag = warp % A, pg = warp / A;
@@ -365,24 +616,8 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
   const float4 *orig = T.lig + (size_t)lig_conf * lna;
   LaneState &me = s_lane[lane];
   const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
-
-  // this warp's atoms; padding atoms use the all-zero table row, no charge,
-  // and sit far from everything
-  int lto[NA];
-  float lq[NA];  // charge / el1: far-field electrostatics is q ele / (el1 d)
-  int n_my = 0;
-#pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    const int a = ag + A * k;
-    if (a < lna) {
-      n_my = k + 1;
-      lto[k] = T.lig_t[a] * GD_NPT;
-      lq[k] = T.lig_q[a];
-    } else {
-      lto[k] = GD_NLT * GD_NPT;
-      lq[k] = 0.f;
-    }
-  }
+  // slots of this warp: ag + A k, k < n_my hold atoms
+  const int n_my = lna > ag ? min(NA, (lna - ag + A - 1) / A) : 0;
 
   if (warp == 0) {
     me.acs = 0;
@@ -395,14 +630,27 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
       for (int i = 0; i < 6; ++i) me.m_old[i] = I.m_old[(size_t)rep * 6 + i];
 #pragma unroll
       for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = I.e_old[(size_t)rep * GD_NTERM + i];
+      me.cmcc_old = I.cmcc ? I.cmcc[rep] : 0.f;
     } else {
 #pragma unroll
       for (int i = 0; i < 6; ++i) me.m_old[i] = 0.f;
 #pragma unroll
       for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = 0.f;
+      me.cmcc_old = 0.f;
     }
+    me.cmcc_new = 0.f;
   }
-  const float lj0 = T.lj0, lj0lj1 = T.lj0lj1, inv_el1 = T.inv_el1, near_d2 = T.near_d2;
+  const float inv_el1 = T.inv_el1;
+  PairConst K;
+  K.one = dup2(1.0f);
+  K.lj1 = dup2(T.lj0lj1);
+  K.lj0 = dup2(T.lj0);
+  K.ca = dup2(-0.5f * LOG2E);
+  K.cb = dup2(6.0f * LOG2E);
+  const float4 *my_ptab = s_ptab + (size_t)ag * NH * PT_ROWS * 2;
+  const float4 *my_htab = s_htab + (size_t)ag * NH * PT_ROWS;
+  const uint32_t *my_hmask = s_hmask + (size_t)ag * PT_ROWS;
+  const bool mcc_on = MODE != KMODE_POSES && (I.flags & GD_MC_MCC) != 0u;
 
   int it = 0;  // streaming ring position
   for (int si = 0; si < n_steps; ++si) {
@@ -441,22 +689,32 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     }
     named_sync(1, W * 32);
 
-    // ---- place this warp's atoms -------------------------------------------
+    // ---- place this warp's atoms (negated: d = atom - point = (-point)... ---
     const float q00 = me.rot[0], q01 = me.rot[1], q02 = me.rot[2];
     const float q10 = me.rot[3], q11 = me.rot[4], q12 = me.rot[5];
     const float q20 = me.rot[6], q21 = me.rot[7], q22 = me.rot[8];
     const float t0 = me.m_new[0], t1 = me.m_new[1], t2 = me.m_new[2];
-    float lx[NA], ly[NA], lz[NA];
+    // nx[h] = {-x of slot 2h, -x of slot 2h+1}: point - atom = px + nx
+    float2 nx[NH], ny[NH], nz[NH];
     // per-atom hydrophobic sums of this warp's tiles live in shared memory
     // (touched only on the close-range path)
-    float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per atom
+    float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per slot
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
-      // padding atoms sit far from everything
-      const float4 o = (k < n_my) ? orig[ag + A * k] : make_float4(FAR, FAR, FAR, 0.f);
-      lx[k] = q00 * o.x + q01 * o.y + q02 * o.z + t0 + lcx;
-      ly[k] = q10 * o.x + q11 * o.y + q12 * o.z + t1 + lcy;
-      lz[k] = q20 * o.x + q21 * o.y + q22 * o.z + t2 + lcz;
+      const float4 o =
+          (k < n_my) ? orig[s_atom[ag + A * k]] : make_float4(FAR, FAR, FAR, 0.f);
+      const float x = q00 * o.x + q01 * o.y + q02 * o.z + t0 + lcx;
+      const float y = q10 * o.x + q11 * o.y + q12 * o.z + t1 + lcy;
+      const float z = q20 * o.x + q21 * o.y + q22 * o.z + t2 + lcz;
+      if (k & 1) {
+        nx[k >> 1].y = -x;
+        ny[k >> 1].y = -y;
+        nz[k >> 1].y = -z;
+      } else {
+        nx[k >> 1].x = -x;
+        ny[k >> 1].x = -y;
+        nz[k >> 1].x = -z;
+      }
       if (k < n_my) my_hpc[(size_t)A * k * 32] = 0.f;
     }
 
@@ -466,125 +724,146 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     double *my_red = s_red + (size_t)warp * NRED * 32 + lane;
 #pragma unroll
     for (int i = 0; i < NRED; ++i) my_red[i * 32] = 0.0;
-    const int t_first = resident ? pg : 0;
-    const int t_step = resident ? P : 1;
-    for (int t = t_first; t < n_tiles; t += t_step, ++it) {
+    // resident: the tile groups take the 32-point chunks round robin
+    // (chunk c to group c mod P), which balances them to within one chunk;
+    // streaming (P = 1): every warp sweeps every tile of the ring
+    constexpr int CPT = TILE_PTS / CHUNK;  // chunks per tile
+    for (int t = 0; t < n_tiles; ++t, ++it) {
+      const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
+      // with PTS == 2 the points are taken in pairs (the padding point that
+      // rounds a tile's point count up to even adds exactly zero), two
+      // blocks per iteration so their independent chains interleave
+      const int nvalid2 = PTS == 2 ? (nvalid + 1) & ~1 : nvalid;
+      const int k0 = resident ? ((pg - (t * CPT) % P) % P + P) % P : 0;
+      const int kstep = resident ? P : 1;
+      if (k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile for this group
       const int s = resident ? t : (it % NS);
       const uint32_t ph = resident ? 0u : (uint32_t)((it / NS) & 1);
       mbar_wait(&s_full[s], ph, R.err, 2);
       const float4 *ta = reinterpret_cast<const float4 *>(s_tiles + (size_t)s * STAGE_BYTES);
       const float2 *tb =
           reinterpret_cast<const float2 *>(s_tiles + (size_t)s * STAGE_BYTES + TILE_PTS * 16);
-      const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
-      for (int j0 = 0; j0 < nvalid; j0 += CHUNK) {
-        const int j1 = min(nvalid, j0 + CHUNK);
-        float fvdw = 0.f, fnear = 0.f, fpmf = 0.f, fpsp = 0.f, fhdb = 0.f;
-        float fek[NA];  // sum of ele_p / d per atom (far-field electrostatics)
+      for (int j0 = k0 * CHUNK; j0 < nvalid2; j0 += kstep * CHUNK) {
+        const int j1 = min(nvalid2, j0 + CHUNK);
+        float2 fvdw = dup2(0.f), fpmf = dup2(0.f), fhdb = dup2(0.f);
+        float fnear = 0.f, fpsp = 0.f;
+        float2 fek[NH];  // sum of ele_p / d per atom (far-field electrostatics)
 #pragma unroll
-        for (int k = 0; k < NA; ++k) fek[k] = 0.f;
-        for (int j = j0; j < j1; ++j) {
-          const float4 Ap = ta[j];
-          const float2 Bp = tb[j];
-          const uint32_t meta = __float_as_uint(Bp.y);
-          const int pt = (int)(meta & META_TYPE_MASK);
-          float mn = 3.0e38f;
-          // fast path: soft LJ, far-field electrostatics, contact PMF.  The LJ
-          // and PMF quotients share one reciprocal: with D1 = p4 and
-          // D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2); d2 >= 1e-6 keeps
-          // D1 D2 below 1e35.
-#pragma unroll
-          for (int k = 0; k < NA; ++k) {
-            const float4 Pk = s_tab_a[lto[k] + pt];  // p1a p2a pmf0 pmf1
-            const float dx = lx[k] - Ap.x;
-            const float dy = ly[k] - Ap.y;
-            const float dz = lz[k] - Ap.z;
-            const float d2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1.0e-6f);
-            const float r = frsqrt(d2);
-            const float d = d2 * r;
-            const float r2 = r * r;
-            const float r3 = r2 * r;
-            const float r6 = r3 * r3;
-            const float r9 = r6 * r3;
-            const float p1 = Pk.x * r9;
-            const float p2 = Pk.y * r6;
-            const float p4 = fmaf(p1, fmaf(lj0lj1, d2, lj0), 1.0f);
-            const float dm = d - Pk.z;
-            const float e1 = 1.0f + fex2(fmaf(-0.5f * LOG2E, d, 6.0f * LOG2E) * dm);
-            const float inv = frcp(p4 * e1);
-            fvdw = fmaf((p1 - p2) * e1, inv, fvdw);
-            fpmf = fmaf(Pk.w * p4, inv, fpmf);
-            fek[k] = fmaf(Ap.w, r, fek[k]);
-            mn = fminf(mn, d2);
-            // hydrogen bond, for the type pairs that define one
-            const float2 Hk = s_tab_b[lto[k] + pt];  // hdb0 hdb1
-            if (Hk.x > 0.1f) {
-              const float h3 = (d - Hk.x) * Hk.y;
-              fhdb = fmaf(Hk.y, fex2((-0.5f * LOG2E) * h3 * h3), fhdb);
-            }
-          }
-          // close-range terms, only when some lane has an atom within near_d2
-          // (distances recomputed: this path is taken for a few % of points)
-          if (__any_sync(0xffffffffu, mn <= near_d2)) {
+        for (int h = 0; h < NH; ++h) fek[h] = dup2(0.f);
+        if (PTS == 1) {
+          for (int j = j0; j < j1; ++j) {
+            const float4 A0 = ta[j];
+            const uint32_t meta = __float_as_uint(tb[j].y);
+            const int pt = (int)(meta & META_TYPE_MASK);
+            const float4 *pp = my_ptab + pt * 2;
+            float mn = 3.0e38f;
+            if (my_hmask[pt] == 0u)
+              pair_block1<NH, false>(nx, ny, nz, A0, pp, nullptr, K, fvdw, fpmf, fhdb, fek, mn);
+            else
+              pair_block1<NH, true>(nx, ny, nz, A0, pp, my_htab + pt, K, fvdw, fpmf, fhdb, fek,
+                                    mn);
             const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
             const bool hflag = (meta & META_HPC_BIT) != 0u;
-#pragma unroll
-            for (int k = 0; k < NA; ++k) {
-              const float dx = lx[k] - Ap.x;
-              const float dy = ly[k] - Ap.y;
-              const float dz = lz[k] - Ap.z;
-              const float d2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1.0e-6f);
-              const float rk = frsqrt(d2);
-              const float d = d2 * rk;
-              if (hflag && d2 <= 81.0f && k < n_my) {
-                float *h = my_hpc + (size_t)A * k * 32;
-                *h = fmaf(Bp.x, hpc_poly(d2), *h);
-              }
-              const float s1 = T.el1 * d;
-              if (s1 < 1.0f) {
-                const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
-                fnear = fmaf(lq[k] * Ap.w, gnear - rk * inv_el1, fnear);
-              }
-              if (is_c2 && k < n_my) {
-                const float dm = d - s_tab_a[lto[k] + pt].z;
-                if (dm <= 0.0f)
-                  fpsp += __ldg(&T.psp[(size_t)(lto[k] / GD_NPT) * T.psp_ncol +
-                                       (meta >> META_SEQ_SHIFT)]);
-              }
-            }
+            float thr = T.near4[(hflag ? 1 : 0) | (is_c2 ? 2 : 0)];
+            if (mcc_on) thr = fmaxf(thr, T.near_mcc2);
+            if (__any_sync(0xffffffffu, mn <= thr))
+              close_range<NA>(nx, ny, nz, A0, tb[j].x, meta, pp, T, s_q, s_lt, s_atom, my_hpc,
+                              A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
+                              my_red);
           }
+        } else {
+        for (int j = j0; j < j1; j += 2) {
+          const float4 A0 = ta[j], A1 = ta[j + 1];
+          const uint32_t meta0 = __float_as_uint(tb[j].y), meta1 = __float_as_uint(tb[j + 1].y);
+          const int pt0 = (int)(meta0 & META_TYPE_MASK), pt1 = (int)(meta1 & META_TYPE_MASK);
+          const float4 *pp0 = my_ptab + pt0 * 2, *pp1 = my_ptab + pt1 * 2;
+          float mn0 = 3.0e38f, mn1 = 3.0e38f;
+          // fast path, branch-free inside; the H-bond variant runs for point
+          // types that form one with some atom of this warp
+          switch ((my_hmask[pt0] != 0u ? 1 : 0) | (my_hmask[pt1] != 0u ? 2 : 0)) {
+            case 0:
+              pair_block2<NH, false, false>(nx, ny, nz, A0, A1, pp0, pp1, nullptr, nullptr, K,
+                                            fvdw, fpmf, fhdb, fek, mn0, mn1);
+              break;
+            case 1:
+              pair_block2<NH, true, false>(nx, ny, nz, A0, A1, pp0, pp1, my_htab + pt0, nullptr,
+                                           K, fvdw, fpmf, fhdb, fek, mn0, mn1);
+              break;
+            case 2:
+              pair_block2<NH, false, true>(nx, ny, nz, A0, A1, pp0, pp1, nullptr, my_htab + pt1,
+                                           K, fvdw, fpmf, fhdb, fek, mn0, mn1);
+              break;
+            default:
+              pair_block2<NH, true, true>(nx, ny, nz, A0, A1, pp0, pp1, my_htab + pt0,
+                                          my_htab + pt1, K, fvdw, fpmf, fhdb, fek, mn0, mn1);
+              break;
+          }
+          // close-range terms, only when some lane has an atom within the
+          // point's threshold (this path is taken for a few % of points)
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const float4 Ap = q ? A1 : A0;
+            const uint32_t meta = q ? meta1 : meta0;
+            const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
+            const bool hflag = (meta & META_HPC_BIT) != 0u;
+            float thr = T.near4[(hflag ? 1 : 0) | (is_c2 ? 2 : 0)];
+            if (mcc_on) thr = fmaxf(thr, T.near_mcc2);
+            if (__any_sync(0xffffffffu, (q ? mn1 : mn0) <= thr))
+              close_range<NA>(nx, ny, nz, Ap, tb[j + q].x, meta, q ? pp1 : pp0, T, s_q, s_lt,
+                              s_atom, my_hpc, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on,
+                              t * TILE_PTS + j + q, my_red);
+          }
+        }
         }
         float fele = 0.f;
 #pragma unroll
-        for (int k = 0; k < NA; ++k) fele = fmaf(lq[k], fek[k], fele);
-        my_red[0 * 32] += (double)fvdw;
+        for (int h = 0; h < NH; ++h) {
+          fele = fmaf(s_q[ag + A * (2 * h)], fek[h].x, fele);
+          fele = fmaf(s_q[ag + A * (2 * h + 1)], fek[h].y, fele);
+        }
+        my_red[0 * 32] += (double)fvdw.x + (double)fvdw.y;
         my_red[1 * 32] += (double)fele * (double)inv_el1 + (double)fnear;
-        my_red[2 * 32] += (double)fpmf;
+        my_red[2 * 32] += (double)fpmf.x + (double)fpmf.y;
         my_red[3 * 32] += (double)fpsp;
-        my_red[4 * 32] += (double)fhdb;
+        my_red[4 * 32] += (double)fhdb.x + (double)fhdb.y;
       }
       if (!resident) {
+        // the last of the W warps to finish this stage refills it with the
+        // tile NS positions later in the sequence
         __syncwarp();
-        if (lane == 0) mbar_arrive(&s_empty[s]);
+        if (lane == 0) {
+          __threadfence_block();
+          if (atomicAdd(&s_done[s], 1) == W - 1) {
+            s_done[s] = 0;
+            __threadfence_block();
+            if (it + NS < n_seq) {
+              fence_proxy_async_smem();
+              issue_tile(it + NS);
+            }
+          }
+        }
       }
     }
 
-    // ---- per-atom hydrophobic sums, KDE --------------------------------------
+    // ---- KDE ------------------------------------------------------------------
     double dkde = 0.0, dlhm = 0.0;
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
-      if (k < n_my) {
-        if (k % P == pg) {
-          const int lt = lto[k] / GD_NPT;
-          const int kb = T.kde_off[lt], ke = T.kde_off[lt + 1];
-          if (ke > kb) {
-            float kv = 0.f;
-            for (int q = kb; q < ke; ++q) {
-              const float4 K = T.kde[q];
-              const float dx = lx[k] - K.x, dy = ly[k] - K.y, dz = lz[k] - K.z;
-              kv += fex2(T.kde2 * LOG2E * fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
-            }
-            dkde += (double)kv / (double)(ke - kb);
+      if (k < n_my && k % P == pg) {
+        const int lt = s_lt[ag + A * k];
+        const int kb = T.kde_off[lt], ke = T.kde_off[lt + 1];
+        if (ke > kb) {
+          const float2 ax = nx[k >> 1], ay = ny[k >> 1], az = nz[k >> 1];
+          const float x = -((k & 1) ? ax.y : ax.x);
+          const float y = -((k & 1) ? ay.y : ay.x);
+          const float z = -((k & 1) ? az.y : az.x);
+          float kv = 0.f;
+          for (int q = kb; q < ke; ++q) {
+            const float4 K = T.kde[q];
+            const float dx = x - K.x, dy = y - K.y, dz = z - K.z;
+            kv += fex2(T.kde2 * LOG2E * fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
           }
+          dkde += (double)kv / (double)(ke - kb);
         }
       }
     }
@@ -613,7 +892,7 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     }
     named_sync(1, W * 32);
     if (warp == 0)
-      finish_step<MODE>(R, I, me, s_red, s_hpc, W, P, MAXA, lane, rep, active, prt_conf,
+      finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, MAXA, lane, rep, active, prt_conf,
                         lig_conf, step);
     // the next step's first barrier orders warp 0's updates (and its use of
     // s_red for the exchange) before any other warp touches them again
@@ -625,6 +904,7 @@ __global__ void __launch_bounds__((MAX_WARPS + 1) * 32, 1)
     for (int i = 0; i < 6; ++i) I.m_old[(size_t)rep * 6 + i] = me.m_old[i];
 #pragma unroll
     for (int i = 0; i < GD_NTERM; ++i) I.e_old[(size_t)rep * GD_NTERM + i] = me.e_old[i];
+    if (I.cmcc) I.cmcc[rep] = me.cmcc_old;
     if (MODE == KMODE_INIT) {
       I.acs_mc[rep] = 0;
       I.idx_tmp[rep] = (rep / I.n_lig_conf) % I.n_tmp;
@@ -647,7 +927,9 @@ __global__ void exchange_kernel(const KItem *items, const KGroup *groups, int n_
   const KItem &I = items[G.item];
   // interval start: the device counter, the launch's step, or (step0 < 0)
   // each item's own step
-  const int s0 = step_ptr ? *step_ptr : (step0 >= 0 ? step0 : I.step0);
+  const bool per_item = !step_ptr && step0 < 0;
+  const int s0 = step_ptr ? *step_ptr : (per_item ? I.step0 : step0);
+  if (per_item) spe = I.spe;
   const int within = I.steps_per_dump > 0 ? (s0 % I.steps_per_dump) : s0;
   const int mode_t = (within / spe) % 2;
   const int round = s0 / spe;
@@ -741,7 +1023,7 @@ __global__ void fma_peak_kernel(float *out, int iters) {
 template <int MODE, int NA>
 static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
   const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages);
-  const int threads = (R.A * R.P + 1) * 32;
+  const int threads = R.A * R.P * 32;
   cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -752,11 +1034,8 @@ static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
 template <int MODE>
 static cudaError_t launch_mode(const KRun &R, int NA, int grid, cudaStream_t s) {
   switch (NA) {
-    case 1: return launch_na<MODE, 1>(R, grid, s);
     case 2: return launch_na<MODE, 2>(R, grid, s);
-    case 3: return launch_na<MODE, 3>(R, grid, s);
     case 4: return launch_na<MODE, 4>(R, grid, s);
-    case 5: return launch_na<MODE, 5>(R, grid, s);
     case 6: return launch_na<MODE, 6>(R, grid, s);
     case 8: return launch_na<MODE, 8>(R, grid, s);
     case 10: return launch_na<MODE, 10>(R, grid, s);

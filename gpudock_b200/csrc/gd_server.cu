@@ -4,8 +4,9 @@
 // server's resident proteins, with its own MC parameters) are queued by
 // gd_server_submit and admitted by a scheduler thread while the HBM budget
 // and the slot count allow.  Every scheduler iteration advances all admitted
-// requests by `steps_per_launch` MC steps in one launch per launch shape:
-// each request keeps its own step counter (KItem.step0), replica state and
+// requests in one launch per launch shape, each by a number of MC steps
+// balanced by its cost (plan_steps): each request keeps its own step counter
+// and step count (KItem.step0 / n_run), replica state and
 // random stream, so requests that arrived at different times share launches
 // and a request's results do not depend on what else is running.  Finished
 // requests are copied out and their memory returns to the budget before the
@@ -15,6 +16,7 @@
 // process, run.cu:41-353); the semantics of every request are those of Run.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -65,9 +67,11 @@ struct Req {
   Clock::time_point t_submit, t_start, t_done;
   // device side while active
   gd_dcomplex *dcx = nullptr;
-  float *d_m_old = nullptr, *d_e_old = nullptr, *d_mb = nullptr;
+  float *d_m_old = nullptr, *d_e_old = nullptr, *d_mb = nullptr, *d_cmcc = nullptr;
   int *d_idx = nullptr, *d_acs = nullptr, *d_acx = nullptr;
   int step = 0;
+  int n_run = 0;      // MC steps of the current iteration
+  double cost = 0.0;  // ligand-size bucket x protein points (time per MC step)
   KItem item{};
   // results
   std::vector<float> energy, movematrix;
@@ -113,7 +117,9 @@ size_t request_bytes(const gd_complex *cx, int n_rep) {
   b += (size_t)GD_NLT * cx->psp.n_col * 4;
   b += (size_t)cx->kde.pnk * 16 + (GD_NLT + 1) * 4;
   b += (size_t)cx->mcs.pos * cx->lig.lna * 16 + (size_t)cx->mcs.pos * 8;
-  b += (size_t)n_rep * (6 + GD_NTERM + 2) * 4 + 3 * MAX_TMP * 4;
+  b += (size_t)n_rep * (6 + GD_NTERM + 3) * 4 + 3 * MAX_TMP * 4;
+  // MCC reference map: one bit per (atom, padded point)
+  b += (size_t)cx->lig.lna * ((cx->prt.pnp + TILE_PTS - 1) / TILE_PTS) * (TILE_PTS / 8);
   return b;
 }
 
@@ -126,6 +132,8 @@ void release_device(gd_server *S, Req *r) {
   cudaStream_t s = S->ctx->stream;
   if (r->d_m_old) cudaFreeAsync(r->d_m_old, s);
   if (r->d_e_old) cudaFreeAsync(r->d_e_old, s);
+  if (r->d_cmcc) cudaFreeAsync(r->d_cmcc, s);
+  r->d_cmcc = nullptr;
   if (r->d_mb) cudaFreeAsync(r->d_mb, s);
   if (r->d_idx) cudaFreeAsync(r->d_idx, s);
   if (r->d_acs) cudaFreeAsync(r->d_acs, s);
@@ -158,6 +166,7 @@ gd_status admit(gd_server *S, Req *r) {
   const size_t n = (size_t)r->n_rep;
   GD_CUDA(cudaMallocAsync(&r->d_m_old, n * 6 * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_e_old, n * GD_NTERM * sizeof(float), s));
+  GD_CUDA(cudaMallocAsync(&r->d_cmcc, n * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_mb, MAX_TMP * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_idx, n * sizeof(int), s));
   GD_CUDA(cudaMallocAsync(&r->d_acs, n * sizeof(int), s));
@@ -174,6 +183,7 @@ gd_status admit(gd_server *S, Req *r) {
   I.n_prt = I.T.n_prt;
   I.n_rep = r->n_rep;
   I.steps_per_dump = r->mc.steps_per_dump;
+  I.spe = r->mc.steps_per_exchange;
   for (int k = 0; k < 6; ++k) I.move_scale[k] = r->mc.move_scale[k];
   I.seed = r->mc.seed;
   I.stream_id = r->mc.stream_id;
@@ -183,9 +193,11 @@ gd_status admit(gd_server *S, Req *r) {
   I.record = nullptr;
   I.m_old = r->d_m_old;
   I.e_old = r->d_e_old;
+  I.cmcc = r->d_cmcc;
   I.idx_tmp = r->d_idx;
   I.acs_mc = r->d_acs;
   r->step = 0;
+  r->cost = (double)lna_bucket(I.T.lna) * I.T.pnp;
   return GD_OK;
 }
 
@@ -207,6 +219,7 @@ gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n
   for (size_t i = 0; i < rs.size(); ++i) {
     Req *r = rs[i];
     r->item.step0 = r->step;
+    r->item.n_run = mode == KMODE_REMC ? r->n_run : 1;
     items.push_back(r->item);
     const KItem &I = r->item;
     Tile t = tile_for(S->ctx, I.T);
@@ -305,8 +318,8 @@ gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n
   }
   GD_TRY(join_streams(S->ctx, n_side));
   if (!groups.empty()) {
-    GD_CUDA(launch_exchange(S->d_items, S->d_groups, (int)groups.size(), S->steps_per_launch, -1,
-                            nullptr, s));
+    // per-item mode (step0 < 0): each group uses its item's step and spe
+    GD_CUDA(launch_exchange(S->d_items, S->d_groups, (int)groups.size(), 1, -1, nullptr, s));
     S->ctx->launches += 1;
     S->n_launch += 1;
   }
@@ -337,6 +350,34 @@ void finish(gd_server *S, Req *r, ReqState st, gd_status err) {
   r->t_done = Clock::now();
   S->bytes_in_use -= r->bytes;
   if (st == RQ_DONE) S->n_done += 1;
+}
+
+// MC steps of every active request in the next iteration.  A request's CTAs
+// take time proportional to its cost per step, so the most expensive request
+// advances steps_per_launch steps (rounded to its exchange interval) and the
+// others proportionally more, in whole exchange intervals and at most their
+// remaining steps: every CTA of the iteration runs about equally long and no
+// request holds the others back.  Requests whose exchange runs as a separate
+// kernel advance one interval.
+void plan_steps(gd_server *S, const std::vector<Req *> &rs) {
+  double quantum = 0.0;
+  for (Req *r : rs) {
+    const int spe = r->mc.steps_per_exchange;
+    const int n = std::max(spe, S->steps_per_launch / spe * spe);
+    quantum = std::max(quantum, r->cost * n);
+  }
+  for (Req *r : rs) {
+    const int spe = r->mc.steps_per_exchange;
+    const int left = r->mc.steps_total - r->step;
+    int n;
+    if ((r->mc.flags & GD_MC_EXCHANGE) && 32 % r->mc.n_tmp != 0) {
+      n = spe;
+    } else {
+      const double k = std::floor(quantum / (r->cost * spe));
+      n = (int)std::min<double>(std::max(1.0, k), (double)(left / spe)) * spe;
+    }
+    r->n_run = std::max(spe, std::min(n, left));
+  }
 }
 
 void scheduler(gd_server *S) {
@@ -395,7 +436,8 @@ void scheduler(gd_server *S) {
     }
     gd_status st = launch_all(S, ok_fresh, KMODE_INIT, 1);
     for (Req *r : ok_fresh) todo.push_back(r);
-    if (st == GD_OK) st = launch_all(S, todo, KMODE_REMC, S->steps_per_launch);
+    plan_steps(S, todo);
+    if (st == GD_OK) st = launch_all(S, todo, KMODE_REMC, 0);
     if (st == GD_OK) {
       cudaEventRecord(S->ev, S->ctx->stream);
       cudaEventSynchronize(S->ev);
@@ -403,7 +445,7 @@ void scheduler(gd_server *S) {
     }
     std::vector<Req *> finished;
     for (Req *r : todo) {
-      r->step += S->steps_per_launch;
+      r->step += r->n_run;
       if (st == GD_OK && r->step >= r->mc.steps_total) {
         if (copy_out(S, r) == GD_OK) finished.push_back(r);
       }
@@ -551,18 +593,11 @@ extern "C" gd_status gd_server_submit(gd_server *S, int protein_id, const gd_com
   }
   if (mc->n_tmp < 1 || mc->n_tmp > MAX_TMP || !mc->minus_beta)
     return fail(GD_EINVAL, "n_tmp=%d", mc->n_tmp);
-  if (mc->steps_per_exchange < 1 || S->steps_per_launch % mc->steps_per_exchange != 0)
-    return fail(GD_EINVAL, "steps_per_exchange %d does not divide the server's %d steps per "
-                "launch", mc->steps_per_exchange, S->steps_per_launch);
-  // without whole exchange groups per CTA the exchange is a separate launch
-  // after each server iteration, so the iteration must be one interval
-  if ((mc->flags & GD_MC_EXCHANGE) && 32 % mc->n_tmp != 0 &&
-      mc->steps_per_exchange != S->steps_per_launch)
-    return fail(GD_EINVAL, "n_tmp=%d needs steps_per_exchange == %d (the server's steps per "
-                "launch)", mc->n_tmp, S->steps_per_launch);
-  if (mc->steps_total < S->steps_per_launch || mc->steps_total % S->steps_per_launch != 0)
-    return fail(GD_EINVAL, "steps_total %d is not a multiple of %d", mc->steps_total,
-                S->steps_per_launch);
+  if (mc->steps_per_exchange < 1)
+    return fail(GD_EINVAL, "steps_per_exchange=%d", mc->steps_per_exchange);
+  if (mc->steps_total < mc->steps_per_exchange || mc->steps_total % mc->steps_per_exchange != 0)
+    return fail(GD_EINVAL, "steps_total %d is not a positive multiple of steps_per_exchange %d",
+                mc->steps_total, mc->steps_per_exchange);
   auto r = std::make_unique<Req>();
   try {
     GD_TRY(copy_request(S, protein_id, cx, mc, r.get()));

@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -444,6 +445,36 @@ def autotune_buckets(dcxs):
         if k not in rep or d.cx.lna > rep[k].cx.lna:
             rep[k] = d
     return {k: d.autotune() for k, d in sorted(rep.items())}
+
+
+def autotune_cadence(ctx: Context, dcxs, minus_beta, candidates=(1, 2, 4, 5, 10, 20, 50),
+                     tol: float = 0.02, steps: int = 100, **kw):
+    """Exchange-cadence autotuner for a batch.
+
+    Exchanging more often mixes the temperature ladder faster but costs a
+    kernel boundary per interval where the exchange cannot run inside the
+    MC kernel.  Each candidate steps_per_exchange is timed on the batch
+    (about `steps` MC steps after a warm-up); the smallest cadence whose time
+    per MC step is within `tol` of the fastest candidate is returned with the
+    table {spe: ms per MC step}.  The cadence changes the sampled trajectory,
+    so the caller decides whether to adopt it."""
+    table = {}
+    for spe in candidates:
+        n = max(spe, (steps // spe) * spe)
+        params = [abi.mc_params(3 * n, spe, minus_beta, stream_id=i, **kw)
+                  for i in range(len(dcxs))]
+        b = Batch(ctx, dcxs, params)
+        b.init()
+        b.run(n)
+        ctx.sync()
+        t0 = time.perf_counter()
+        b.run(n)
+        ctx.sync()
+        table[spe] = (time.perf_counter() - t0) * 1e3 / n
+        b.close()
+    best = min(table.values())
+    chosen = min(s for s, t in table.items() if t <= best * (1.0 + tol))
+    return chosen, table
 
 
 def fma_peak(ctx: Context, n_blocks: int = 148 * 16, iters: int = 4096):

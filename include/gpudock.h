@@ -238,9 +238,11 @@ typedef struct gd_tile {
   int atoms_per_warp;
 } gd_tile;
 
-/* Times every compiled launch shape for this complex's size class on one
- * wave of pose CTAs, keeps the fastest in the context and returns it; later
- * launches of that size class use it.  A size class is (ligand-size bucket,
+/* Times every compiled launch shape for this complex's size class on the
+ * REMC kernel (a temporary batch of copies of the complex, one CTA per SM or
+ * more, a few MC steps per sample), keeps the fastest in the context and
+ * returns it with its time for 4 MC steps; later launches of that size class
+ * use it.  Synchronous; takes about a second.  A size class is (ligand-size bucket,
  * protein tiles): ligand sizes are rounded up to a multiple of 8 atoms and a
  * class's shape covers the bucket's largest size, so the ligands of a batch
  * that fall in one bucket share one launch shape. */
@@ -300,6 +302,15 @@ gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *dcx,
 #define GD_MC_EXCHANGE   0x1u  /* temperature exchange (IS_EXCHANGE)        */
 #define GD_MC_MOVE_AWAY  0x2u  /* initial MoveAway_d + forced accept        */
 #define GD_MC_RECORD     0x4u  /* per-step trajectory record (IS_OUTPUT)    */
+/* Contact-map Matthews correlation of every pose (IS_CALCU_MCC,
+ * calcmcc_d.cu:57-213): contacts are ligand-atom / protein-point pairs with
+ * d <= pmf0; the reference map is that of ligand conformation 0 in its start
+ * pose against the complex's first protein conformation.  Per step
+ * cmcc = (tp tn - fp fn) / sqrt((tp+fp)(tp+fn)(tn+fp)(tn+fn)), or 10000 when
+ * the denominator is 0.  It follows the accepted state and is reported in
+ * gd_record.cmcc; it never enters the acceptance. */
+#define GD_MC_MCC        0x8u
+#define GD_CMCC_INVALID  10000.0f
 
 typedef struct gd_mc_params {
   int steps_total;           /* MC steps per replica                        */
@@ -400,9 +411,13 @@ gd_status gd_batch_kernel_times(gd_batch *batch, double *mc_ms, int *mc_launches
 /* uploaded once and stay resident; requests (a ligand ensemble + pocket    */
 /* template + MC parameters against a resident protein) are copied at       */
 /* submit, admitted by a scheduler thread while the HBM budget and the      */
-/* slot count allow, and advanced together steps_per_launch MC steps per    */
-/* iteration, each with its own step counter, state and random stream, so  */
-/* a request's result does not depend on what else is running.              */
+/* slot count allow, and advanced together in iterations, each with its own */
+/* step counter, state and random stream, so a request's result does not    */
+/* depend on what else is running.  In an iteration the most expensive      */
+/* active request (ligand atoms x protein points) advances steps_per_launch */
+/* MC steps (at least one exchange interval) and cheaper ones               */
+/* proportionally more, in whole exchange intervals, so that no request     */
+/* holds the others back.                                                   */
 /* ------------------------------------------------------------------------ */
 typedef struct gd_server gd_server;
 

@@ -408,11 +408,91 @@ void orc_energy_poses(const gd_complex *cx, int prt_conf, int lig_conf, int n,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Contact-map MCC (calcmcc_d.cu): InitRefMatrix_d :57-83, CalcMcc_d        */
+/* :148-213.  ref[l * pnp + p] = 1 where dst <= pmf0 for ligand conformation */
+/* 0 in its start pose against protein conformation prt_conf.               */
+/* ------------------------------------------------------------------------ */
+static void orc_contacts(const gd_complex *cx, int prt_conf, const float *lx,
+                         const float *ly, const float *lz, unsigned char *out)
+{
+  const gd_protein *pr = &cx->prt;
+  const int pnp = pr->pnp;
+  for (int l = 0; l < cx->lig.lna; ++l) {
+    const int lt = cx->lig.t[l];
+    for (int p = 0; p < pnp; ++p) {
+      const size_t i = (size_t)prt_conf * pnp + p;
+      const float dx = lx[l] - pr->x[i];
+      const float dy = ly[l] - pr->y[i];
+      const float dz = lz[l] - pr->z[i];
+      const float dst = sqrtf(dx * dx + dy * dy + dz * dz);
+      out[(size_t)l * pnp + p] = dst <= cx->ff->pmf0[lt][pr->t[p]];
+    }
+  }
+}
+
+static unsigned char *orc_mcc_ref(const gd_complex *cx, int prt_conf, int *nref)
+{
+  const int lna = cx->lig.lna;
+  unsigned char *ref = (unsigned char *)malloc((size_t)lna * cx->prt.pnp);
+  float *buf = (float *)malloc(sizeof(float) * 3 * (size_t)lna);
+  for (int l = 0; l < lna; ++l) {
+    buf[l] = cx->lig.x[l] + cx->lig.center[0];
+    buf[lna + l] = cx->lig.y[l] + cx->lig.center[1];
+    buf[2 * lna + l] = cx->lig.z[l] + cx->lig.center[2];
+  }
+  orc_contacts(cx, prt_conf, buf, buf + lna, buf + 2 * lna, ref);
+  int n = 0;
+  for (size_t i = 0; i < (size_t)lna * cx->prt.pnp; ++i) n += ref[i];
+  *nref = n;
+  free(buf);
+  return ref;
+}
+
+static float orc_mcc_of(const gd_complex *cx, int prt_conf, const float *lx,
+                        const float *ly, const float *lz,
+                        const unsigned char *ref)
+{
+  const size_t n = (size_t)cx->lig.lna * cx->prt.pnp;
+  unsigned char *cur = (unsigned char *)malloc(n);
+  orc_contacts(cx, prt_conf, lx, ly, lz, cur);
+  int tp = 0, fn = 0, fpc = 0, tn = 0;
+  for (size_t i = 0; i < n; ++i) {
+    tp += ref[i] == 1 && cur[i];
+    fn += ref[i] == 1 && !cur[i];
+    fpc += ref[i] == 0 && cur[i];
+    tn += ref[i] == 0 && !cur[i];
+  }
+  free(cur);
+  const float tp0 = (float)tp, fn0 = (float)fn, fp0 = (float)fpc, tn0 = (float)tn;
+  const float dividend = sqrtf((tp0 + fp0) * (tp0 + fn0) * (tn0 + fp0) * (tn0 + fn0));
+  return dividend != 0.0f ? (tp0 * tn0 - fp0 * fn0) / dividend : GD_CMCC_INVALID;
+}
+
+/* MCC of one pose (move vector m of ligand conformation lig_conf against
+ * protein conformation prt_conf), with the reference map of the complex
+ * (ligand conformation 0, start pose, protein conformation ref_prt). */
+float orc_mcc(const gd_complex *cx, int ref_prt, int prt_conf, int lig_conf,
+              const float m[6])
+{
+  int nref;
+  unsigned char *ref = orc_mcc_ref(cx, ref_prt, &nref);
+  const int lna = cx->lig.lna;
+  float *buf = (float *)malloc(sizeof(float) * 3 * (size_t)lna);
+  float center[3];
+  orc_place(cx, lig_conf, m, buf, buf + lna, buf + 2 * lna, center);
+  const float v = orc_mcc_of(cx, prt_conf, buf, buf + lna, buf + 2 * lna, ref);
+  free(buf);
+  free(ref);
+  return v;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Replica-exchange Monte Carlo                                             */
 /* ------------------------------------------------------------------------ */
 typedef struct orc_rep {
   float m_old[6];
   float e_old[GD_NTERM];
+  float cmcc;
   int idx_tmp;
   int acs;
 } orc_rep;
@@ -421,7 +501,7 @@ typedef struct orc_rep {
  * proposed total energy through *e_prop and the decision. */
 static int orc_mc_step(const gd_complex *cx, const gd_mc_params *mc, int n_lig,
                        int n_tmp, int r, int step, orc_rep *st, float *buf,
-                       float *e_prop)
+                       float *e_prop, const unsigned char *mcc_ref)
 {
   const int p = r / (n_tmp * n_lig);
   const int l = r % n_lig;
@@ -451,6 +531,8 @@ static int orc_mc_step(const gd_complex *cx, const gd_mc_params *mc, int n_lig,
   if (acc) {
     memcpy(st->m_old, m_new, sizeof(m_new));
     memcpy(st->e_old, e_new, sizeof(e_new));
+    /* MCC follows the accepted state (accept_d.cu:50) */
+    if (mcc_ref) st->cmcc = orc_mcc_of(cx, p, buf, buf + lna, buf + 2 * lna, mcc_ref);
     st->acs += 1;
   }
   return acc;
@@ -534,6 +616,10 @@ int orc_remc_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log,
   const int lna = cx->lig.lna;
   orc_rep *reps = (orc_rep *)calloc((size_t)n_rep, sizeof(orc_rep));
   int *acs_slot = (int *)calloc((size_t)n_tmp, sizeof(int));
+  /* MCC reference map from replica 0 before MoveAway (montecarlo_d.cu:24-25) */
+  int nref = 0;
+  unsigned char *mcc_ref =
+      (mc->flags & GD_MC_MCC) ? orc_mcc_ref(cx, 0, &nref) : NULL;
 #ifdef _OPENMP
   if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -561,6 +647,7 @@ int orc_remc_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log,
       double raw[GD_NRAW];
       orc_energy_coords(cx, p, buf, buf + lna, buf + 2 * lna, center, raw,
                         st->e_old, NULL);
+      st->cmcc = mcc_ref ? orc_mcc_of(cx, p, buf, buf + lna, buf + 2 * lna, mcc_ref) : 0.0f;
       /* forced accept with beta = 0 (montecarlo_d.cu:236-239) */
       memcpy(st->m_old, m, sizeof(m));
       st->acs = 0;
@@ -587,13 +674,13 @@ int orc_remc_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log,
             rec.idx_tmp = reps[r].idx_tmp;
             rec.idx_lig = l;
             memcpy(rec.e, reps[r].e_old, sizeof(rec.e));
-            rec.cmcc = 0.0f;
+            rec.cmcc = mcc_ref ? reps[r].cmcc : 0.0f;
             memcpy(rec.movematrix, reps[r].m_old, sizeof(rec.movematrix));
             rec.step = s;
           }
           float e_prop;
           const int acc =
-              orc_mc_step(cx, mc, n_lig, n_tmp, r, s, &reps[r], buf, &e_prop);
+              orc_mc_step(cx, mc, n_lig, n_tmp, r, s, &reps[r], buf, &e_prop, mcc_ref);
           if (log && log->record) {
             rec.e_prop_total = e_prop;
             rec.accepted = acc;
@@ -632,6 +719,7 @@ int orc_remc_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log,
   }
   free(reps);
   free(acs_slot);
+  free(mcc_ref);
   return GD_OK;
 }
 
@@ -660,7 +748,7 @@ long long orc_mc_sample(const gd_complex *cx, const gd_mc_params *mc, int r0,
       st.e_old[GD_E_TOTAL] = 0.0f;
       for (int s = 0; s < n_steps; ++s) {
         float e_prop;
-        orc_mc_step(cx, mc, n_lig, n_tmp, r, s, &st, buf, &e_prop);
+        orc_mc_step(cx, mc, n_lig, n_tmp, r, s, &st, buf, &e_prop, NULL);
         done += 1;
       }
     }

@@ -57,6 +57,8 @@ def load(native: bool = False):
                                   C.c_int, C.c_int, C.c_int]
     lib.orc_mc_sample.restype = C.c_longlong
     lib.orc_max_threads.restype = C.c_int
+    lib.orc_mcc.argtypes = [C.POINTER(abi.GdComplex), C.c_int, C.c_int, C.c_int, P]
+    lib.orc_mcc.restype = C.c_float
     _libs[key] = lib
     return lib
 
@@ -145,3 +147,11 @@ def mc_sample(cx: abi.Complex, params: abi.GdMcParams, r0: int, n_rep: int, n_st
 
 def max_threads(native: bool = False) -> int:
     return int(load(native).orc_max_threads())
+
+
+def mcc(cx: abi.Complex, ref_prt: int, prt_conf: int, lig_conf: int, m) -> float:
+    """Contact MCC of the pose m (6-vector) against the complex's reference
+    map (ligand conformation 0, start pose, protein conformation ref_prt)."""
+    mv = np.ascontiguousarray(m, np.float32).reshape(6)
+    return float(load().orc_mcc(C.byref(cx.struct()), ref_prt, prt_conf, lig_conf,
+                                mv.ctypes.data))

@@ -115,6 +115,26 @@ def test_oracle_remc_runs_and_counts():
     assert (rec["step"] == np.arange(40)).all()
 
 
+def test_oracle_mcc_bookkeeping():
+    """GD_MC_MCC in the oracle's REMC driver: every recorded value is the MCC of
+    the recorded (accepted) pose; the start pose of ligand conformation 0 against
+    protein conformation 0 is the reference map itself (MCC 1); the score never
+    changes the trajectory."""
+    cx = synth.make_complex(synth.ComplexSpec(pnp=300, lna=10, n_prt=2, n_lig=2), seed=6)
+    _, mb = lib.set_temperature(4, 0.01, 0.05)
+    assert orc.mcc(cx, 0, 0, 0, np.zeros(6)) == 1.0
+    base = abi.MC_EXCHANGE | abi.MC_RECORD | abi.MC_MOVE_AWAY
+    a = orc.remc_run(cx, 20, 5, mb, seed=4, flags=base)
+    b = orc.remc_run(cx, 20, 5, mb, seed=4, flags=base | abi.MC_MCC)
+    assert np.array_equal(a.energy, b.energy) and np.all(a.record["cmcc"] == 0)
+    rec = b.record
+    for r in range(0, rec.shape[0], 3):
+        for s in (0, 7, 19):
+            x = rec[r, s]
+            assert x["cmcc"] == orc.mcc(cx, 0, int(x["idx_prt"]), int(x["idx_lig"]),
+                                        x["movematrix"])
+
+
 def test_exchange_rules():
     """Pairing of exchangereplicas_d.cu:43-46: (0,1),(2,3).. for mode 0,
     (1,2),(3,4).. for mode 1; an infinitely favourable swap always happens."""
