@@ -379,16 +379,32 @@ extern "C" gd_status gd_complex_free(gd_dcomplex *d) {
 extern "C" size_t gd_complex_device_bytes(const gd_dcomplex *d) { return d ? d->bytes : 0; }
 
 // Packs the protein conformations into {x, y, z, ele} and {hpp, meta}.
-static gd_status upload_protein(const gd_protein &P, gd_dcomplex *d) {
+// The device order of the points: those whose type forms an H-bond with
+// some ligand type (hdb0 > 0.1) first, each kind in the caller's order.  The
+// energy is a sum over points, so the order changes nothing but the FP32
+// rounding inside a 32-point chunk.
+static gd_status upload_protein(const gd_protein &P, const gd_enepara &F, gd_dcomplex *d) {
   KTables &T = d->T;
   const int pnp = P.pnp;
   const int pnp_pad = (pnp + TILE_PTS - 1) / TILE_PTS * TILE_PTS;
+  bool hb_type[GD_NPT];
+  for (int j = 0; j < GD_NPT; ++j) {
+    hb_type[j] = false;
+    for (int i = 0; i < GD_NLT; ++i) hb_type[j] = hb_type[j] || F.hdb0[i][j] > 0.1f;
+  }
+  std::vector<int> &order = d->point_order;
+  order.clear();
+  order.reserve(pnp);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int p = 0; p < pnp; ++p)
+      if (hb_type[P.t[p]] == (pass == 0)) order.push_back(p);
   std::vector<float4> pa((size_t)P.n_conf * pnp_pad,
                          make_float4(PAD_POINT_COORD, PAD_POINT_COORD, PAD_POINT_COORD, 0.f));
   for (int c = 0; c < P.n_conf; ++c)
-    for (int p = 0; p < pnp; ++p) {
+    for (int s = 0; s < pnp; ++s) {
+      const int p = order[s];
       const size_t i = (size_t)c * pnp + p;
-      pa[(size_t)c * pnp_pad + p] = make_float4(P.x[i], P.y[i], P.z[i], P.ele[p]);
+      pa[(size_t)c * pnp_pad + s] = make_float4(P.x[i], P.y[i], P.z[i], P.ele[p]);
     }
   float pad_meta;
   {
@@ -396,13 +412,14 @@ static gd_status upload_protein(const gd_protein &P, gd_dcomplex *d) {
     std::memcpy(&pad_meta, &m, 4);
   }
   std::vector<float2> pb((size_t)pnp_pad, make_float2(0.f, pad_meta));
-  for (int p = 0; p < pnp; ++p) {
+  for (int s = 0; s < pnp; ++s) {
+    const int p = order[s];
     uint32_t meta = (uint32_t)P.t[p] | ((uint32_t)P.c[p] << META_CLASS_SHIFT) |
                     ((uint32_t)P.seq3r[p] << META_SEQ_SHIFT);
     if (P.c0_and_d12_or_c2[p] == 1) meta |= META_HPC_BIT;
     float mf;
     std::memcpy(&mf, &meta, 4);
-    pb[p] = make_float2(P.hpp[p], mf);
+    pb[s] = make_float2(P.hpp[p], mf);
   }
   GD_TRY(upload(d, pa, &T.pt_a));
   GD_TRY(upload(d, pb, &T.pt_b));
@@ -497,6 +514,7 @@ static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
     if (kind & 2) r = std::max(r, max_pmf0);
     T.near4[kind] = r * r * 1.0001f + 1e-3f;
   }
+  T.near_ele2 = F.el1 > 0.f ? r_ele * r_ele * 1.0001f + 1e-3f : 1e30f;
   // kernel slot order: atoms with an H-bond term (some point type with
   // hdb0 > 0.1) first, so that they share atom pairs and warps
   std::vector<int> order;
@@ -536,6 +554,10 @@ static gd_status upload_mcc_ref(const gd_complex *cx, int prt_conf, gd_dcomplex 
   KTables &T = d->T;
   const int words = T.pnp_pad / 32;
   const int pc = prt_conf < P.n_conf ? prt_conf : 0;
+  // bits are indexed by the device position of a point
+  const std::vector<int> &order =
+      d->protein_owner ? d->protein_owner->point_order : d->point_order;
+  if ((int)order.size() != P.pnp) return fail(GD_EINVAL, "protein point order missing");
   std::vector<uint32_t> bits((size_t)L.lna * words, 0u);
   int nref = 0;
   float max_pmf0 = 0.f;
@@ -545,14 +567,15 @@ static gd_status upload_mcc_ref(const gd_complex *cx, int prt_conf, gd_dcomplex 
     const float lx = L.x[a] + L.center[0];
     const float ly = L.y[a] + L.center[1];
     const float lz = L.z[a] + L.center[2];
-    for (int p = 0; p < P.pnp; ++p) {
+    for (int s = 0; s < P.pnp; ++s) {
+      const int p = order[s];
       const size_t i = (size_t)pc * P.pnp + p;
       const float dx = lx - P.x[i];
       const float dy = ly - P.y[i];
       const float dz = lz - P.z[i];
       const float dst = sqrtf(dx * dx + dy * dy + dz * dz);
       if (dst <= F.pmf0[L.t[a]][P.t[p]]) {
-        bits[(size_t)a * words + (p >> 5)] |= 1u << (p & 31);
+        bits[(size_t)a * words + (s >> 5)] |= 1u << (s & 31);
         ++nref;
       }
     }
@@ -595,7 +618,7 @@ static gd_status complex_upload_common(gd_ctx *ctx, const gd_complex *cx,
       d->T.pnp_pad = share->T.pnp_pad;
       d->T.n_prt = n_prt;
     } else {
-      st = upload_protein(cx->prt, d);
+      st = upload_protein(cx->prt, *cx->ff, d);
     }
     if (st == GD_OK) st = upload_ligand(cx, d);
     if (st == GD_OK) st = upload_mcc_ref(cx, share ? prt_conf0 : 0, d);

@@ -79,6 +79,9 @@ struct gd_dcomplex {
   size_t bytes = 0;
   std::atomic<int> refs{1};
   gd_dcomplex *protein_owner = nullptr;  // when the protein arrays are shared
+  // device position -> caller's point index: points whose type can form an
+  // H-bond come first, so a 32-point chunk rarely mixes the two kinds
+  std::vector<int> point_order;
 };
 
 namespace gd {

@@ -61,6 +61,9 @@ struct KTables {
   int lna, n_lig, pnp, pnp_pad, n_prt, pos, psp_ncol, mcc_words;
   float mcc_nref;       // contacts in the reference map
   float near_mcc2;      // squared distance within which a contact can occur
+                        // (max pmf0^2, with margin)
+  float near_ele2;      // squared distance of the near-field electrostatics
+                        // switch (1/el1)^2, with margin
   float lj0, lj0lj1, el0, el1, inv_el1, a1, b1, kde2, kde3;
   float s2pi;           // sqrtf(2 * 3.1415926535f), the reference's float
   float near4[4];       // squared distance below which a close-range term can

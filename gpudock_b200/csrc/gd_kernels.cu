@@ -47,13 +47,6 @@ constexpr float FAR = 1.0e4f;  // coordinate of the padding atoms
 // all-zero rows, one of which (PAD_POINT_TYPE) marks the padding points that
 // fill a tile past the protein's last point, so they add exactly zero.
 constexpr int PT_ROWS = 32;
-// Largest atoms-per-warp count whose pair loop takes two protein points per
-// iteration (more independent work per warp); above it the registers do not
-// allow the second point.
-#ifndef GD_PTS2_MAX_NA
-#define GD_PTS2_MAX_NA 4
-#endif
-constexpr int PTS2_MAX_NA = GD_PTS2_MAX_NA;
 static_assert(PAD_POINT_TYPE >= GD_NPT && PAD_POINT_TYPE < PT_ROWS, "padding type row");
 
 // Per-replica state in shared memory, written by warp 0 only.
@@ -402,22 +395,30 @@ __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2
     pair_hh<HDB>(nx[h], ny[h], nz[h], A0, pp, hp, h, K, fvdw, fpmf, fhdb, fek[h], mn);
 }
 
-// Two protein points (A0, A1) against this lane's NA atoms.  The body has no
-// branches, so the compiler interleaves the 2 x NA/2 independent chains; the
-// sums keep the order point A0 before A1 for every atom pair.
-template <int NH, bool HDB0, bool HDB1>
-__device__ __forceinline__ void pair_block2(const float2 (&nx)[NH], const float2 (&ny)[NH],
-                                            const float2 (&nz)[NH], const float4 &A0,
-                                            const float4 &A1, const float4 *pp0,
-                                            const float4 *pp1, const float4 *hp0,
-                                            const float4 *hp1, const PairConst &K, float2 &fvdw,
-                                            float2 &fpmf, float2 &fhdb, float2 (&fek)[NH],
-                                            float &mn0, float &mn1) {
-#pragma unroll
-  for (int h = 0; h < NH; ++h) {
-    pair_hh<HDB0>(nx[h], ny[h], nz[h], A0, pp0, hp0, h, K, fvdw, fpmf, fhdb, fek[h], mn0);
-    pair_hh<HDB1>(nx[h], ny[h], nz[h], A1, pp1, hp1, h, K, fvdw, fpmf, fhdb, fek[h], mn1);
+// The fast path over points j0 .. j1-1 of a staged tile, one point per
+// iteration and no branch in the body, so the compiler can overlap one
+// point's tail with the next point's head.  Returns the mask of points whose
+// close-range terms must run: some lane has an atom within the point's
+// threshold (thr_l, held by lane j - j0).
+template <int NH, bool HDB>
+__device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const float2 (&ny)[NH],
+                                               const float2 (&nz)[NH], const float4 *ta,
+                                               const float2 *tb, int j0, int j1,
+                                               const float4 *my_ptab, const float4 *my_htab,
+                                               const PairConst &K, float thr_l, float2 &fvdw,
+                                               float2 &fpmf, float2 &fhdb, float2 (&fek)[NH]) {
+  uint32_t close = 0u;
+#pragma unroll 2
+  for (int j = j0; j < j1; ++j) {
+    const float4 Ap = ta[j];
+    const int pt = (int)(__float_as_uint(tb[j].y) & META_TYPE_MASK);
+    float mn = 3.0e38f;
+    pair_block1<NH, HDB>(nx, ny, nz, Ap, my_ptab + pt * 2, my_htab + pt, K, fvdw, fpmf, fhdb,
+                         fek, mn);
+    const float thr = __shfl_sync(0xffffffffu, thr_l, j - j0);
+    close |= (__any_sync(0xffffffffu, mn <= thr) ? 1u : 0u) << (j - j0);
   }
+  return close;
 }
 
 // Close-range terms of one protein point (calcenergy_d.cu:80-138): the
@@ -449,14 +450,18 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
       float *hh = my_hpc + (size_t)A * k * 32;
       *hh = fmaf(hpp, hpc_poly(d2), *hh);
     }
-    const float rk = frsqrt(d2);
-    const float d = d2 * rk;
-    const float s1 = T.el1 * d;
-    if (s1 < 1.0f) {
-      const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
-      fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
+    // the distance itself only where a switch can be near (d^2 bounds with
+    // margin: the tests below decide on d exactly as before)
+    if (d2 <= T.near_ele2) {
+      const float rk = frsqrt(d2);
+      const float s1 = T.el1 * (d2 * rk);
+      if (s1 < 1.0f) {
+        const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
+        fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
+      }
     }
-    if ((is_c2 || mcc_on) && k < n_my) {
+    if ((is_c2 || mcc_on) && k < n_my && d2 <= T.near_mcc2) {
+      const float d = d2 * frsqrt(d2);
       const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
       const float dm = d + ((k & 1) ? T1.y : T1.x);
       if (dm <= 0.0f) {
@@ -481,8 +486,6 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     dock_kernel(const __grid_constant__ KRun R) {
   static_assert(NA % 2 == 0, "atoms are processed in pairs");
   constexpr int NH = NA / 2;
-  // protein points per loop iteration: two while the registers allow
-  constexpr int PTS = NA <= PTS2_MAX_NA ? 2 : 1;
   extern __shared__ __align__(128) unsigned char smem[];
   const int A = R.A, P = R.P, W = A * P, NS = R.n_stages;
   const int MAXA = A * NA;
@@ -730,10 +733,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     constexpr int CPT = TILE_PTS / CHUNK;  // chunks per tile
     for (int t = 0; t < n_tiles; ++t, ++it) {
       const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
-      // with PTS == 2 the points are taken in pairs (the padding point that
-      // rounds a tile's point count up to even adds exactly zero), two
-      // blocks per iteration so their independent chains interleave
-      const int nvalid2 = PTS == 2 ? (nvalid + 1) & ~1 : nvalid;
+      const int nvalid2 = nvalid;
       const int k0 = resident ? ((pg - (t * CPT) % P) % P + P) % P : 0;
       const int kstep = resident ? P : 1;
       if (k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile for this group
@@ -750,70 +750,29 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         float2 fek[NH];  // sum of ele_p / d per atom (far-field electrostatics)
 #pragma unroll
         for (int h = 0; h < NH; ++h) fek[h] = dup2(0.f);
-        if (PTS == 1) {
-          for (int j = j0; j < j1; ++j) {
-            const float4 A0 = ta[j];
-            const uint32_t meta = __float_as_uint(tb[j].y);
-            const int pt = (int)(meta & META_TYPE_MASK);
-            const float4 *pp = my_ptab + pt * 2;
-            float mn = 3.0e38f;
-            if (my_hmask[pt] == 0u)
-              pair_block1<NH, false>(nx, ny, nz, A0, pp, nullptr, K, fvdw, fpmf, fhdb, fek, mn);
-            else
-              pair_block1<NH, true>(nx, ny, nz, A0, pp, my_htab + pt, K, fvdw, fpmf, fhdb, fek,
-                                    mn);
-            const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
-            const bool hflag = (meta & META_HPC_BIT) != 0u;
-            float thr = T.near4[(hflag ? 1 : 0) | (is_c2 ? 2 : 0)];
-            if (mcc_on) thr = fmaxf(thr, T.near_mcc2);
-            if (__any_sync(0xffffffffu, mn <= thr))
-              close_range<NA>(nx, ny, nz, A0, tb[j].x, meta, pp, T, s_q, s_lt, s_atom, my_hpc,
-                              A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
-                              my_red);
-          }
-        } else {
-        for (int j = j0; j < j1; j += 2) {
-          const float4 A0 = ta[j], A1 = ta[j + 1];
-          const uint32_t meta0 = __float_as_uint(tb[j].y), meta1 = __float_as_uint(tb[j + 1].y);
-          const int pt0 = (int)(meta0 & META_TYPE_MASK), pt1 = (int)(meta1 & META_TYPE_MASK);
-          const float4 *pp0 = my_ptab + pt0 * 2, *pp1 = my_ptab + pt1 * 2;
-          float mn0 = 3.0e38f, mn1 = 3.0e38f;
-          // fast path, branch-free inside; the H-bond variant runs for point
-          // types that form one with some atom of this warp
-          switch ((my_hmask[pt0] != 0u ? 1 : 0) | (my_hmask[pt1] != 0u ? 2 : 0)) {
-            case 0:
-              pair_block2<NH, false, false>(nx, ny, nz, A0, A1, pp0, pp1, nullptr, nullptr, K,
-                                            fvdw, fpmf, fhdb, fek, mn0, mn1);
-              break;
-            case 1:
-              pair_block2<NH, true, false>(nx, ny, nz, A0, A1, pp0, pp1, my_htab + pt0, nullptr,
-                                           K, fvdw, fpmf, fhdb, fek, mn0, mn1);
-              break;
-            case 2:
-              pair_block2<NH, false, true>(nx, ny, nz, A0, A1, pp0, pp1, nullptr, my_htab + pt1,
-                                           K, fvdw, fpmf, fhdb, fek, mn0, mn1);
-              break;
-            default:
-              pair_block2<NH, true, true>(nx, ny, nz, A0, A1, pp0, pp1, my_htab + pt0,
-                                          my_htab + pt1, K, fvdw, fpmf, fhdb, fek, mn0, mn1);
-              break;
-          }
-          // close-range terms, only when some lane has an atom within the
-          // point's threshold (this path is taken for a few % of points)
-#pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const float4 Ap = q ? A1 : A0;
-            const uint32_t meta = q ? meta1 : meta0;
-            const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
-            const bool hflag = (meta & META_HPC_BIT) != 0u;
-            float thr = T.near4[(hflag ? 1 : 0) | (is_c2 ? 2 : 0)];
-            if (mcc_on) thr = fmaxf(thr, T.near_mcc2);
-            if (__any_sync(0xffffffffu, (q ? mn1 : mn0) <= thr))
-              close_range<NA>(nx, ny, nz, Ap, tb[j + q].x, meta, q ? pp1 : pp0, T, s_q, s_lt,
-                              s_atom, my_hpc, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on,
-                              t * TILE_PTS + j + q, my_red);
-          }
-        }
+        // the chunk's variant of the fast path: with the H-bond term when one
+        // of its points has a type that forms one with an atom of this warp
+        // (points are ordered so that chunks rarely mix the two kinds); the
+        // close-range votes are collected in a mask and served after the
+        // branch-free pass, so consecutive points' chains overlap
+        const int jl = j0 + lane;
+        const uint32_t meta_l = jl < j1 ? __float_as_uint(tb[jl].y) : (uint32_t)PAD_POINT_TYPE;
+        const bool chunk_hdb = __any_sync(0xffffffffu, my_hmask[meta_l & META_TYPE_MASK] != 0u);
+        float thr_l = T.near4[((meta_l & META_HPC_BIT) ? 1 : 0) |
+                              ((((meta_l >> META_CLASS_SHIFT) & 3u) == 2u) ? 2 : 0)];
+        if (mcc_on) thr_l = fmaxf(thr_l, T.near_mcc2);
+        const uint32_t close =
+            chunk_hdb ? chunk_fast<NH, true>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
+                                             thr_l, fvdw, fpmf, fhdb, fek)
+                      : chunk_fast<NH, false>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
+                                              thr_l, fvdw, fpmf, fhdb, fek);
+        for (uint32_t m = close; m != 0u; m &= m - 1u) {
+          const int j = j0 + __ffs(m) - 1;
+          const uint32_t meta = __float_as_uint(tb[j].y);
+          close_range<NA>(nx, ny, nz, ta[j], tb[j].x, meta,
+                          my_ptab + (int)(meta & META_TYPE_MASK) * 2, T, s_q, s_lt, s_atom,
+                          my_hpc, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
+                          my_red);
         }
         float fele = 0.f;
 #pragma unroll
