@@ -294,13 +294,16 @@ def form_served(seed, rate=50.0, n_request=300, steps=2000, budget_gb=120):
             time.sleep(dt)
         ids.append(srv.submit(pids[which[i]], cx, steps, w.steps_per_exchange, mb, n_prt=1,
                               seed=seed, stream_id=i, flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY))
-    lat = []
+    lat, svc = [], []
     for rid in ids:
-        lat.append(srv.wait(rid, timeout_ms=900000).log.t_wall)
+        log = srv.wait(rid, timeout_ms=900000).log
+        lat.append(log.t_wall)
+        svc.append(log.t_compute)
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
     lat = np.asarray(lat)
+    svc = np.asarray(svc)
     n_rep = 32
     return {"workload": w.name, "n_request": n_request, "rate_req_s": rate,
             "mc_steps": steps, "replicas_per_request": n_rep,
@@ -308,6 +311,8 @@ def form_served(seed, rate=50.0, n_request=300, steps=2000, budget_gb=120):
             "requests_per_s": n_request / wall,
             "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)),
+            "p50_service_s": float(np.percentile(svc, 50)),
+            "p99_service_s": float(np.percentile(svc, 99)),
             "busy_s": st.busy_s, "launches": st.launches,
             "sample": f"{n_request} of the 10,000-request trace at {rate:g} req/s"}
 

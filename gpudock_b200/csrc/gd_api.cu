@@ -44,9 +44,9 @@ int round_na(int na) {
 }
 
 // Default launch shape (used until the autotuner has timed a size class):
-// atom groups to cover the ligand, and when the protein is resident as many
-// tile groups as fit in MAX_WARPS.
-Tile default_tile(int lna, bool resident) {
+// atom groups to cover the ligand and as many tile groups as fit in
+// MAX_WARPS (resident or streamed, the groups split the protein's chunks).
+Tile default_tile(int lna) {
   // A warp's time per protein point is about NA + 1.5 pair-slots (its atoms
   // plus the per-point loads and test), and the A x P warps share the points
   // P ways: pick the shape with the smallest (NA + 1.5) / P.
@@ -56,7 +56,7 @@ Tile default_tile(int lna, bool resident) {
     const int A = (lna + na - 1) / na;
     if (A > MAX_WARPS) continue;
     const int NA = round_na((lna + A - 1) / A);
-    const int P = resident ? std::max(1, MAX_WARPS / A) : 1;
+    const int P = std::max(1, MAX_WARPS / A);
     const double cost = (NA + 1.5) / P;
     if (cost < best_cost - 1e-9) {
       best_cost = cost;
@@ -80,12 +80,6 @@ void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident) 
   }
 }
 
-static bool fits_resident(const KTables &T, const Tile &t) {
-  const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
-  return n_tiles <= MAX_RESIDENT_TILES &&
-         dock_smem_bytes(t.A, t.P, t.NA, n_tiles) <= 227 * 1024;
-}
-
 int lna_bucket(int lna) { return std::min(((lna + 7) / 8) * 8, MAX_LNA); }
 
 Tile tile_for(gd_ctx *ctx, const KTables &T) {
@@ -96,9 +90,7 @@ Tile tile_for(gd_ctx *ctx, const KTables &T) {
     auto it = ctx->tiles.find({hi, n_tiles});
     if (it != ctx->tiles.end()) return it->second;
   }
-  Tile t = default_tile(hi, true);
-  if (!fits_resident(T, t)) t = default_tile(hi, false);
-  return t;
+  return default_tile(hi);
 }
 
 void ctx_retain(gd_ctx *c) {
@@ -154,13 +146,15 @@ void dcx_retain(gd_dcomplex *d) {
   if (d) d->refs++;
 }
 
+// The last reference frees the tables in stream order on the context stream
+// (work of the library's side streams is joined into it; the server frees a
+// request only after its lane's launches have ended).
 void dcx_release(gd_dcomplex *d) {
   if (!d || --d->refs > 0) return;
   if (d->ctx) {
     cudaSetDevice(d->ctx->device);
-    cudaStreamSynchronize(d->ctx->stream);
+    for (void *p : d->allocs) cudaFreeAsync(p, d->ctx->stream);
   }
-  for (void *p : d->allocs) cudaFree(p);
   gd_ctx *c = d->ctx;
   gd_dcomplex *owner = d->protein_owner;
   delete d;
@@ -357,11 +351,15 @@ extern "C" uint64_t gd_ctx_launch_count(const gd_ctx *c) { return c ? c->launche
 // ---------------------------------------------------------------------------
 // Device layout of a complex
 // ---------------------------------------------------------------------------
+// Stream-ordered allocation on the context stream: neither this nor the
+// matching cudaFreeAsync in dcx_release synchronises the device, so a
+// server uploading and releasing requests never stalls the kernels of other
+// streams.
 template <typename T>
 static gd_status upload(gd_dcomplex *d, const std::vector<T> &h, const T **out) {
   void *p = nullptr;
   const size_t n = std::max<size_t>(h.size(), 1) * sizeof(T);
-  GD_CUDA(cudaMalloc(&p, n));
+  GD_CUDA(cudaMallocAsync(&p, n, d->ctx->stream));
   d->allocs.push_back(p);
   d->bytes += n;
   if (!h.empty())
@@ -659,7 +657,6 @@ static gd_status poses_launch(gd_ctx *ctx, const gd_dcomplex *d, const Tile &til
   R.A = tile.A;
   R.P = tile.P;
   pick_stages(d->T, tile, &R.n_stages, &R.resident);
-  if (!R.resident) R.P = 1;
   R.prt_conf = prt_conf;
   R.lig_conf = lig_conf;
   R.n_pose = n_pose;

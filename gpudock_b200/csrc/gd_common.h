@@ -46,7 +46,7 @@ struct Tile {
 // Even: the pair loop handles two atoms per packed f32x2 instruction.
 constexpr int kNAValues[] = {2, 4, 6, 8, 10};
 
-Tile default_tile(int lna, bool resident);
+Tile default_tile(int lna);
 int round_na(int na);  // smallest compiled NA >= na (0 if none)
 void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident);
 

@@ -196,7 +196,6 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     Tile t = tile_for(ctx, I.T);
     int ns, res;
     pick_stages(I.T, t, &ns, &res);
-    if (!res) t.P = 1;
     const int nt = I.n_tmp, nl = I.n_lig_conf;
     const bool gm = (32 % nt) == 0;
     const bool exch = (I.flags & GD_MC_EXCHANGE) != 0;
@@ -703,9 +702,6 @@ extern "C" gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *d, gd_tile *bes
       t.P = P;
       t.NA = na;
       if (A * P < 4 && A * P * 2 <= MAX_WARPS) continue;  // too few warps per SM
-      int ns, res;
-      pick_stages(T, t, &ns, &res);
-      if (!res && P > 1) continue;
       {
         std::lock_guard<std::mutex> g(ctx->tile_mu);
         ctx->tiles[key] = t;

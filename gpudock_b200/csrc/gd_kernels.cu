@@ -728,15 +728,16 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
 #pragma unroll
     for (int i = 0; i < NRED; ++i) my_red[i * 32] = 0.0;
     // resident: the tile groups take the 32-point chunks round robin
-    // (chunk c to group c mod P), which balances them to within one chunk;
-    // streaming (P = 1): every warp sweeps every tile of the ring
+    // (chunk c to group c mod P), which balances them to within one chunk.
+    // Streaming: the same split of every tile of the ring, and every warp
+    // waits for every stage and reports it done, chunk or not
     constexpr int CPT = TILE_PTS / CHUNK;  // chunks per tile
     for (int t = 0; t < n_tiles; ++t, ++it) {
       const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
       const int nvalid2 = nvalid;
-      const int k0 = resident ? ((pg - (t * CPT) % P) % P + P) % P : 0;
-      const int kstep = resident ? P : 1;
-      if (k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile for this group
+      const int k0 = ((pg - (t * CPT) % P) % P + P) % P;
+      const int kstep = P;
+      if (resident && k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile here
       const int s = resident ? t : (it % NS);
       const uint32_t ph = resident ? 0u : (uint32_t)((it / NS) & 1);
       mbar_wait(&s_full[s], ph, R.err, 2);

@@ -89,7 +89,6 @@ extern "C" gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *d, 
   R.A = tile.A;
   R.P = tile.P;
   gd::pick_stages(d->T, tile, &R.n_stages, &R.resident);
-  if (!R.resident) R.P = 1;
   R.prt_conf = prt_conf;
   R.lig_conf = lig_conf;
   R.n_pose = n_pose;

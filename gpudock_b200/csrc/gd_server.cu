@@ -3,14 +3,15 @@
 // Docking requests (a ligand ensemble + pocket template against one of the
 // server's resident proteins, with its own MC parameters) are queued by
 // gd_server_submit and admitted by a scheduler thread while the HBM budget
-// and the slot count allow.  Every scheduler iteration advances all admitted
-// requests in one launch per launch shape, each by a number of MC steps
-// balanced by its cost (plan_steps): each request keeps its own step counter
-// and step count (KItem.step0 / n_run), replica state and
-// random stream, so requests that arrived at different times share launches
-// and a request's results do not depend on what else is running.  Finished
-// requests are copied out and their memory returns to the budget before the
-// next iteration admits more.
+// and the slot count allow.  Requests are grouped by launch shape into lanes,
+// each with its own stream; a lane advances all its requests in one launch,
+// each by a number of MC steps balanced by its cost (plan_steps), and is
+// relaunched as soon as that launch ends, with the requests admitted in the
+// meantime joining it; lanes never wait for one another.  Each request keeps
+// its own step counter and step count (KItem.step0 / n_run), replica state
+// and random stream, so requests that arrived at different times share
+// launches and a request's results do not depend on what else is running.
+// Finished requests are copied out and their memory returns to the budget.
 //
 // There is no counterpart in the reference (Run() handles one complex per
 // process, run.cu:41-353); the semantics of every request are those of Run.
@@ -50,6 +51,8 @@ struct SrvProtein {
   size_t bytes = 0;
 };
 
+struct Lane;
+
 struct Req {
   uint64_t id = 0;
   int protein = 0;
@@ -69,14 +72,42 @@ struct Req {
   gd_dcomplex *dcx = nullptr;
   float *d_m_old = nullptr, *d_e_old = nullptr, *d_mb = nullptr, *d_cmcc = nullptr;
   int *d_idx = nullptr, *d_acs = nullptr, *d_acx = nullptr;
+  Lane *lane = nullptr;            // its launch shape
+  cudaStream_t stream = nullptr;  // the lane's stream
   int step = 0;
-  int n_run = 0;      // MC steps of the current iteration
+  int n_run = 0;      // MC steps of the current launch
   double cost = 0.0;  // ligand-size bucket x protein points (time per MC step)
   KItem item{};
   // results
   std::vector<float> energy, movematrix;
   std::vector<int> acs, idx, acx;
 };
+
+// A launch shape of the server (tile, staging, group layout, exchange
+// interval) with its own stream.  The requests of a lane advance together in
+// rolling launches; lanes never wait for one another, so a shape whose
+// requests are cheap is relaunched as soon as its own kernel ends while
+// other shapes are still running.
+struct Lane {
+  Tile tile;
+  int ns = 0, res = 0, gm = 0, spe = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  int *d_err = nullptr;             // the lane's kernel error word
+  int *h_err = nullptr;             // pinned copy, read after `done`
+  bool busy = false;                // a launch is in flight
+  std::vector<Req *> members;       // active requests of this shape
+  std::vector<Req *> fresh;         // admitted, not yet initialised
+  std::vector<Req *> in_flight;     // the requests of the launch in flight
+  // launch descriptors, grown on demand (reused: one launch at a time)
+  KItem *d_items = nullptr;
+  int *d_cta = nullptr;  // [3][cap_cta]
+  KGroup *d_groups = nullptr;
+  size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
+};
+
+using LaneKey = std::tuple<int, int, int, int, int, int, int>;
+constexpr int kMaxLanes = 256;
 
 }  // namespace
 
@@ -100,12 +131,11 @@ struct gd_server {
   // statistics
   uint64_t n_done = 0, n_iter = 0, n_launch = 0;
   double busy_s = 0.0;
-  // device staging for the launch descriptors, grown on demand
-  KItem *d_items = nullptr;
-  int *d_cta = nullptr;  // [3][cap_cta]
-  KGroup *d_groups = nullptr;
-  size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
-  cudaEvent_t ev = nullptr;
+  // scheduler-thread state
+  std::map<LaneKey, std::unique_ptr<Lane>> lanes;
+  // error words of the lanes (device, zeroed) and their pinned host copies,
+  // allocated once with the server
+  int *d_err_pool = nullptr, *h_err_pool = nullptr;
 };
 
 namespace {
@@ -128,17 +158,16 @@ std::vector<T> vcopy(const T *p, size_t n) {
   return p ? std::vector<T>(p, p + n) : std::vector<T>();
 }
 
-void release_device(gd_server *S, Req *r) {
-  cudaStream_t s = S->ctx->stream;
+void release_device(Req *r) {
+  cudaStream_t s = r->stream;
   if (r->d_m_old) cudaFreeAsync(r->d_m_old, s);
   if (r->d_e_old) cudaFreeAsync(r->d_e_old, s);
   if (r->d_cmcc) cudaFreeAsync(r->d_cmcc, s);
-  r->d_cmcc = nullptr;
   if (r->d_mb) cudaFreeAsync(r->d_mb, s);
   if (r->d_idx) cudaFreeAsync(r->d_idx, s);
   if (r->d_acs) cudaFreeAsync(r->d_acs, s);
   if (r->d_acx) cudaFreeAsync(r->d_acx, s);
-  r->d_m_old = r->d_e_old = r->d_mb = nullptr;
+  r->d_m_old = r->d_e_old = r->d_mb = r->d_cmcc = nullptr;
   r->d_idx = r->d_acs = r->d_acx = nullptr;
   if (r->dcx) {
     cudaStreamSynchronize(s);
@@ -147,22 +176,60 @@ void release_device(gd_server *S, Req *r) {
   }
 }
 
+// Grows a lane's descriptor buffer in stream order on the lane's stream (no
+// device-wide synchronisation while other lanes run).
 template <typename T>
-gd_status grow(T **p, size_t *cap, size_t need) {
+gd_status grow(T **p, size_t *cap, size_t need, cudaStream_t s) {
   if (need <= *cap) return GD_OK;
   size_t n = std::max<size_t>(need, *cap * 2 + 64);
-  if (*p) cudaFree(*p);
+  if (*p) cudaFreeAsync(*p, s);
   *p = nullptr;
-  GD_CUDA(cudaMalloc(p, n * sizeof(T)));
+  GD_CUDA(cudaMallocAsync((void **)p, n * sizeof(T), s));
   *cap = n;
   return GD_OK;
 }
 
-// Uploads the request's tables, allocates its state and fills its KItem.
+// The lane of a request's launch shape, created on first use.
+gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
+  const KTables &T = r->dcx->T;
+  Tile t = tile_for(S->ctx, T);
+  int ns, res;
+  pick_stages(T, t, &ns, &res);
+  const bool gm = (32 % r->mc.n_tmp) == 0;
+  const int spe = r->mc.steps_per_exchange;
+  const LaneKey key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe};
+  auto it = S->lanes.find(key);
+  if (it != S->lanes.end()) {
+    *out = it->second.get();
+    return GD_OK;
+  }
+  auto L = std::make_unique<Lane>();
+  L->tile = t;
+  L->ns = ns;
+  L->res = res;
+  L->gm = gm ? 1 : 0;
+  L->spe = spe;
+  const int slot = (int)S->lanes.size();
+  if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d launch shapes in the server", kMaxLanes);
+  GD_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
+  GD_CUDA(cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming));
+  L->d_err = S->d_err_pool + slot;
+  L->h_err = S->h_err_pool + slot;
+  *out = L.get();
+  S->lanes[key] = std::move(L);
+  return GD_OK;
+}
+
+// Uploads the request's tables, allocates its state on its lane's stream and
+// fills its KItem.
 gd_status admit(gd_server *S, Req *r) {
   SrvProtein &P = *S->proteins[r->protein];
   GD_TRY(gd_complex_upload_shared(S->ctx, &r->cx, P.dcx, 0, P.prt.n_conf, &r->dcx));
-  cudaStream_t s = S->ctx->stream;
+  Lane *L = nullptr;
+  GD_TRY(lane_for(S, r, &L));
+  r->lane = L;
+  r->stream = L->stream;
+  cudaStream_t s = L->stream;
   const size_t n = (size_t)r->n_rep;
   GD_CUDA(cudaMallocAsync(&r->d_m_old, n * 6 * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_e_old, n * GD_NTERM * sizeof(float), s));
@@ -201,20 +268,15 @@ gd_status admit(gd_server *S, Req *r) {
   return GD_OK;
 }
 
-struct ShapePlan {
-  Tile tile;
-  int ns = 0, res = 0, gm = 0, spe = 0;
-  std::vector<std::tuple<double, int, int, int>> ctas;  // cost, item, rep0/group, n
-};
-
-// One launch per launch shape over the given requests (KRun item_step).
-gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n_steps) {
+// One launch of a lane over the given requests (KRun item_step: each request
+// at its own step, for its own step count), plus the exchange kernel for
+// groups that do not fit a CTA.  Asynchronous on the lane's stream.
+gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int mode) {
   if (rs.empty()) return GD_OK;
-  cudaStream_t s = S->ctx->stream;
+  cudaStream_t s = L.stream;
   std::vector<KItem> items;
   items.reserve(rs.size());
-  using Key = std::tuple<int, int, int, int, int, int, int>;
-  std::map<Key, ShapePlan> plans;
+  std::vector<std::tuple<double, int, int, int>> ctas;  // cost, item, rep0/group, n
   std::vector<KGroup> groups;
   for (size_t i = 0; i < rs.size(); ++i) {
     Req *r = rs[i];
@@ -222,143 +284,81 @@ gd_status launch_all(gd_server *S, const std::vector<Req *> &rs, int mode, int n
     r->item.n_run = mode == KMODE_REMC ? r->n_run : 1;
     items.push_back(r->item);
     const KItem &I = r->item;
-    Tile t = tile_for(S->ctx, I.T);
-    int ns, res;
-    pick_stages(I.T, t, &ns, &res);
-    if (!res) t.P = 1;
     const int nt = I.n_tmp, nl = I.n_lig_conf;
-    const bool gm = (32 % nt) == 0;
-    const int spe = r->mc.steps_per_exchange;
-    ShapePlan &pl = plans[Key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe}];
-    pl.tile = t;
-    pl.ns = ns;
-    pl.res = res;
-    pl.gm = gm ? 1 : 0;
-    pl.spe = spe;
-    const double cost = (double)I.T.lna * I.T.pnp;
-    if (gm) {
+    if (L.gm) {
       const int G = 32 / nt;
       for (int p = 0; p < I.n_prt; ++p)
         for (int l0 = 0; l0 < nl; l0 += G)
-          pl.ctas.emplace_back(cost, (int)i, p * nl + l0, std::min(G, nl - l0) * nt);
+          ctas.emplace_back(r->cost * r->item.n_run, (int)i, p * nl + l0,
+                            std::min(G, nl - l0) * nt);
     } else {
       const int per_p = nt * nl;
       for (int p = 0; p < I.n_prt; ++p)
         for (int j = 0; j < per_p; j += 32)
-          pl.ctas.emplace_back(cost, (int)i, p * per_p + j, std::min(32, per_p - j));
+          ctas.emplace_back(r->cost * r->item.n_run, (int)i, p * per_p + j,
+                            std::min(32, per_p - j));
       if (mode == KMODE_REMC && (I.flags & GD_MC_EXCHANGE))
         for (int p = 0; p < I.n_prt; ++p)
           for (int l = 0; l < nl; ++l) groups.push_back(KGroup{(int)i, p, l, 0});
     }
   }
-  size_t n_cta = 0;
-  for (auto &kv : plans) n_cta += kv.second.ctas.size();
-  GD_TRY(grow(&S->d_items, &S->cap_items, items.size()));
-  GD_TRY(grow(&S->d_cta, &S->cap_cta, 3 * n_cta));
-  GD_TRY(grow(&S->d_groups, &S->cap_groups, std::max<size_t>(groups.size(), 1)));
-  // the descriptors of the previous launch may still be read: order the
-  // copies after it on the same stream (pageable copies stage synchronously)
-  GD_CUDA(cudaMemcpyAsync(S->d_items, items.data(), items.size() * sizeof(KItem),
-                          cudaMemcpyHostToDevice, s));
+  // costliest CTAs first, so the longest ones start first
+  std::stable_sort(ctas.begin(), ctas.end(),
+                   [](const auto &a, const auto &b) { return std::get<0>(a) > std::get<0>(b); });
+  const size_t n_cta = ctas.size();
+  GD_TRY(grow(&L.d_items, &L.cap_items, items.size(), s));
+  GD_TRY(grow(&L.d_cta, &L.cap_cta, 3 * n_cta, s));
+  GD_TRY(grow(&L.d_groups, &L.cap_groups, std::max<size_t>(groups.size(), 1), s));
   std::vector<int> cta(3 * n_cta);
-  size_t off = 0;
-  std::vector<std::pair<const ShapePlan *, size_t>> launches;
-  for (auto &kv : plans) {
-    ShapePlan &pl = kv.second;
-    std::stable_sort(pl.ctas.begin(), pl.ctas.end(),
-                     [](const auto &a, const auto &b) { return std::get<0>(a) > std::get<0>(b); });
-    launches.emplace_back(&pl, off);
-    for (size_t c = 0; c < pl.ctas.size(); ++c) {
-      cta[off + c] = std::get<1>(pl.ctas[c]);
-      cta[n_cta + off + c] = std::get<2>(pl.ctas[c]);
-      cta[2 * n_cta + off + c] = std::get<3>(pl.ctas[c]);
-    }
-    off += pl.ctas.size();
+  for (size_t c = 0; c < n_cta; ++c) {
+    cta[c] = std::get<1>(ctas[c]);
+    cta[n_cta + c] = std::get<2>(ctas[c]);
+    cta[2 * n_cta + c] = std::get<3>(ctas[c]);
   }
-  GD_CUDA(cudaMemcpyAsync(S->d_cta, cta.data(), cta.size() * sizeof(int), cudaMemcpyHostToDevice,
+  // the lane's previous launch has ended, and pageable copies stage
+  // synchronously, so the descriptors can be reused
+  GD_CUDA(cudaMemcpyAsync(L.d_items, items.data(), items.size() * sizeof(KItem),
+                          cudaMemcpyHostToDevice, s));
+  GD_CUDA(cudaMemcpyAsync(L.d_cta, cta.data(), cta.size() * sizeof(int), cudaMemcpyHostToDevice,
                           s));
   if (!groups.empty())
-    GD_CUDA(cudaMemcpyAsync(S->d_groups, groups.data(), groups.size() * sizeof(KGroup),
+    GD_CUDA(cudaMemcpyAsync(L.d_groups, groups.data(), groups.size() * sizeof(KGroup),
                             cudaMemcpyHostToDevice, s));
-  // the shapes run side by side on side streams, costliest issued first
-  auto plan_cost = [](const ShapePlan *p) {
-    double c = 0.0;
-    for (const auto &t : p->ctas) c += std::get<0>(t);
-    return c;
-  };
-  std::stable_sort(launches.begin(), launches.end(), [&](const auto &a, const auto &b) {
-    return plan_cost(a.first) > plan_cost(b.first);
-  });
-  const int n_side = std::min((int)launches.size(), kMaxSide);
-  cudaStream_t ss[kMaxSide];
-  GD_TRY(fork_streams(S->ctx, n_side, ss));
-  for (size_t k = 0; k < launches.size(); ++k) {
-    const auto &lp = launches[k];
-    const ShapePlan &pl = *lp.first;
-    KRun R{};
-    R.mode = mode;
-    R.A = pl.tile.A;
-    R.P = pl.tile.P;
-    R.n_stages = pl.ns;
-    R.resident = pl.res;
-    R.items = S->d_items;
-    R.cta_item = S->d_cta + lp.second;
-    R.cta_rep0 = S->d_cta + n_cta + lp.second;
-    R.cta_nrep = S->d_cta + 2 * n_cta + lp.second;
-    R.group_major = pl.gm;
-    R.fused_exchange = pl.gm;
-    R.spe = pl.spe;  // every request of a launch shares its exchange interval
-    R.step0 = 0;
-    R.n_steps = n_steps;
-    R.item_step = 1;
-    R.err = S->ctx->d_err;
-    GD_CUDA(launch_dock(R, pl.tile.NA, (int)pl.ctas.size(), ss[k % n_side]));
-    S->ctx->launches += 1;
-    S->n_launch += 1;
-  }
-  GD_TRY(join_streams(S->ctx, n_side));
+  KRun R{};
+  R.mode = mode;
+  R.A = L.tile.A;
+  R.P = L.tile.P;
+  R.n_stages = L.ns;
+  R.resident = L.res;
+  R.items = L.d_items;
+  R.cta_item = L.d_cta;
+  R.cta_rep0 = L.d_cta + n_cta;
+  R.cta_nrep = L.d_cta + 2 * n_cta;
+  R.group_major = L.gm;
+  R.fused_exchange = L.gm;
+  R.spe = L.spe;
+  R.step0 = 0;
+  R.n_steps = 0;  // per item (item_step)
+  R.item_step = 1;
+  R.err = L.d_err;
+  GD_CUDA(launch_dock(R, L.tile.NA, (int)n_cta, s));
+  S->ctx->launches += 1;
+  S->n_launch += 1;
   if (!groups.empty()) {
     // per-item mode (step0 < 0): each group uses its item's step and spe
-    GD_CUDA(launch_exchange(S->d_items, S->d_groups, (int)groups.size(), 1, -1, nullptr, s));
+    GD_CUDA(launch_exchange(L.d_items, L.d_groups, (int)groups.size(), 1, -1, nullptr, s));
     S->ctx->launches += 1;
     S->n_launch += 1;
   }
   return GD_OK;
 }
 
-gd_status copy_out(gd_server *S, Req *r) {
-  cudaStream_t s = S->ctx->stream;
-  const size_t n = (size_t)r->n_rep;
-  r->energy.resize(n * GD_NTERM);
-  r->movematrix.resize(n * 6);
-  r->acs.resize(n);
-  r->idx.resize(n);
-  r->acx.resize(r->mc.n_tmp);
-  GD_CUDA(cudaMemcpyAsync(r->energy.data(), r->d_e_old, n * GD_NTERM * 4, cudaMemcpyDeviceToHost,
-                          s));
-  GD_CUDA(cudaMemcpyAsync(r->movematrix.data(), r->d_m_old, n * 24, cudaMemcpyDeviceToHost, s));
-  GD_CUDA(cudaMemcpyAsync(r->acs.data(), r->d_acs, n * 4, cudaMemcpyDeviceToHost, s));
-  GD_CUDA(cudaMemcpyAsync(r->idx.data(), r->d_idx, n * 4, cudaMemcpyDeviceToHost, s));
-  GD_CUDA(cudaMemcpyAsync(r->acx.data(), r->d_acx, r->mc.n_tmp * 4, cudaMemcpyDeviceToHost, s));
-  return GD_OK;
-}
-
-void finish(gd_server *S, Req *r, ReqState st, gd_status err) {
-  release_device(S, r);
-  r->state = st;
-  r->err = err;
-  r->t_done = Clock::now();
-  S->bytes_in_use -= r->bytes;
-  if (st == RQ_DONE) S->n_done += 1;
-}
-
-// MC steps of every active request in the next iteration.  A request's CTAs
-// take time proportional to its cost per step, so the most expensive request
-// advances steps_per_launch steps (rounded to its exchange interval) and the
-// others proportionally more, in whole exchange intervals and at most their
-// remaining steps: every CTA of the iteration runs about equally long and no
-// request holds the others back.  Requests whose exchange runs as a separate
-// kernel advance one interval.
+// MC steps of every request of a lane's next launch.  A request's CTAs take
+// time proportional to its cost per step, so the most expensive one advances
+// steps_per_launch steps (rounded to its exchange interval) and the others
+// proportionally more, in whole exchange intervals and at most their
+// remaining steps: the launch's CTAs run about equally long.  Requests whose
+// exchange runs as a separate kernel advance one interval.
 void plan_steps(gd_server *S, const std::vector<Req *> &rs) {
   double quantum = 0.0;
   for (Req *r : rs) {
@@ -380,94 +380,192 @@ void plan_steps(gd_server *S, const std::vector<Req *> &rs) {
   }
 }
 
+gd_status copy_out(Req *r) {
+  cudaStream_t s = r->stream;
+  const size_t n = (size_t)r->n_rep;
+  r->energy.resize(n * GD_NTERM);
+  r->movematrix.resize(n * 6);
+  r->acs.resize(n);
+  r->idx.resize(n);
+  r->acx.resize(r->mc.n_tmp);
+  GD_CUDA(cudaMemcpyAsync(r->energy.data(), r->d_e_old, n * GD_NTERM * 4, cudaMemcpyDeviceToHost,
+                          s));
+  GD_CUDA(cudaMemcpyAsync(r->movematrix.data(), r->d_m_old, n * 24, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->acs.data(), r->d_acs, n * 4, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->idx.data(), r->d_idx, n * 4, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaMemcpyAsync(r->acx.data(), r->d_acx, r->mc.n_tmp * 4, cudaMemcpyDeviceToHost, s));
+  GD_CUDA(cudaStreamSynchronize(s));
+  return GD_OK;
+}
+
+// Called with S->mu held.
+void finish(gd_server *S, Req *r, ReqState st, gd_status err) {
+  release_device(r);
+  r->state = st;
+  r->err = err;
+  r->t_done = Clock::now();
+  S->bytes_in_use -= r->bytes;
+  if (st == RQ_DONE) S->n_done += 1;
+  S->active.erase(std::remove(S->active.begin(), S->active.end(), r), S->active.end());
+}
+
+// The scheduler thread.  Each round it admits queued requests while the HBM
+// budget and the slot count allow, collects the lanes whose launch has ended
+// (advancing their requests, finishing the completed ones), and relaunches
+// every idle lane with its current members plus the newly admitted requests
+// of its shape (initialised first, on the same stream).
 void scheduler(gd_server *S) {
   cudaSetDevice(S->ctx->device);
-  std::unique_lock<std::mutex> lk(S->mu);
-  while (!S->stop) {
-    // drop cancelled requests still in the queue
-    for (auto it = S->queue.begin(); it != S->queue.end();) {
-      if ((*it)->cancel) {
-        (*it)->state = RQ_CANCELLED;
-        (*it)->t_done = Clock::now();
-        it = S->queue.erase(it);
-        S->done_cv.notify_all();
-      } else {
-        ++it;
+  auto t_busy = Clock::now();
+  bool was_busy = false;
+  for (;;) {
+    std::vector<Req *> admitted;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      if (S->stop) break;
+      for (auto it = S->queue.begin(); it != S->queue.end();) {
+        if ((*it)->cancel) {
+          (*it)->state = RQ_CANCELLED;
+          (*it)->t_done = Clock::now();
+          it = S->queue.erase(it);
+          S->done_cv.notify_all();
+        } else {
+          ++it;
+        }
+      }
+      while (!S->queue.empty() &&
+             (S->max_active <= 0 || (int)S->active.size() < S->max_active) &&
+             S->protein_bytes + S->bytes_in_use + S->queue.front()->bytes <= S->budget) {
+        Req *r = S->queue.front();
+        S->queue.pop_front();
+        S->bytes_in_use += r->bytes;
+        r->state = RQ_ACTIVE;
+        r->t_start = Clock::now();
+        S->active.push_back(r);
+        admitted.push_back(r);
+      }
+      bool any = !S->active.empty();
+      if (!any && admitted.empty()) {
+        if (was_busy) {
+          S->busy_s += std::chrono::duration<double>(Clock::now() - t_busy).count();
+          was_busy = false;
+        }
+        S->cv.wait_for(lk, std::chrono::milliseconds(20));
+        continue;
+      }
+      if (!was_busy) {
+        t_busy = Clock::now();
+        was_busy = true;
       }
     }
-    // admit while slots and HBM budget allow (first come, first served)
-    std::vector<Req *> fresh;
-    while (!S->queue.empty() &&
-           (S->max_active <= 0 || (int)(S->active.size() + fresh.size()) < S->max_active) &&
-           S->protein_bytes + S->bytes_in_use + S->queue.front()->bytes <= S->budget) {
-      Req *r = S->queue.front();
-      S->queue.pop_front();
-      S->bytes_in_use += r->bytes;
-      r->state = RQ_ACTIVE;
-      r->t_start = Clock::now();
-      fresh.push_back(r);
-    }
-    if (fresh.empty() && S->active.empty()) {
-      S->cv.wait_for(lk, std::chrono::milliseconds(50));
-      continue;
-    }
-    // cancelled active requests leave at the iteration boundary
-    for (auto it = S->active.begin(); it != S->active.end();) {
-      if ((*it)->cancel) {
-        finish(S, *it, RQ_CANCELLED, GD_ECANCELLED);
-        it = S->active.erase(it);
-        S->done_cv.notify_all();
-      } else {
-        ++it;
-      }
-    }
-    std::vector<Req *> todo = S->active;
-    lk.unlock();
-
-    const auto t0 = Clock::now();
-    std::vector<Req *> ok_fresh;
+    // uploads and state of the admitted requests (outside the lock)
     std::vector<std::pair<Req *, gd_status>> failed;
-    for (Req *r : fresh) {
+    for (Req *r : admitted) {
       gd_status st = admit(S, r);
       if (st == GD_OK)
-        ok_fresh.push_back(r);
+        r->lane->fresh.push_back(r);
       else
         failed.emplace_back(r, st);
     }
-    gd_status st = launch_all(S, ok_fresh, KMODE_INIT, 1);
-    for (Req *r : ok_fresh) todo.push_back(r);
-    plan_steps(S, todo);
-    if (st == GD_OK) st = launch_all(S, todo, KMODE_REMC, 0);
-    if (st == GD_OK) {
-      cudaEventRecord(S->ev, S->ctx->stream);
-      cudaEventSynchronize(S->ev);
-      st = ctx_check(S->ctx);
-    }
+    bool progressed = !admitted.empty();
     std::vector<Req *> finished;
-    for (Req *r : todo) {
-      r->step += r->n_run;
-      if (st == GD_OK && r->step >= r->mc.steps_total) {
-        if (copy_out(S, r) == GD_OK) finished.push_back(r);
+    std::vector<std::pair<Req *, gd_status>> lane_failed;
+    for (auto &kv : S->lanes) {
+      Lane &L = *kv.second;
+      if (L.busy) {
+        const cudaError_t q = cudaEventQuery(L.done);
+        if (q == cudaErrorNotReady) continue;
+        L.busy = false;
+        progressed = true;
+        gd_status st = GD_OK;
+        if (q != cudaSuccess) {
+          st = fail(GD_ECUDA, "server launch: %s", cudaGetErrorString(q));
+        } else if (*L.h_err != 0) {
+          st = fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)",
+                    *L.h_err);
+          *L.h_err = 0;
+          cudaMemsetAsync(L.d_err, 0, sizeof(int), L.stream);
+        }
+        for (Req *r : L.in_flight) {
+          if (st != GD_OK) {
+            lane_failed.emplace_back(r, st);
+            continue;
+          }
+          r->step += r->n_run;
+          if (r->step >= r->mc.steps_total) {
+            const gd_status cs = copy_out(r);
+            if (cs == GD_OK)
+              finished.push_back(r);
+            else
+              lane_failed.emplace_back(r, cs);
+          }
+        }
+        std::vector<Req *> keep;
+        for (Req *r : L.members) {
+          bool gone = std::find(finished.begin(), finished.end(), r) != finished.end();
+          for (auto &f : lane_failed) gone = gone || f.first == r;
+          if (!gone) keep.push_back(r);
+        }
+        L.members.swap(keep);
+        L.in_flight.clear();
       }
     }
-    if (!finished.empty()) cudaStreamSynchronize(S->ctx->stream);
-
-    lk.lock();
-    S->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
-    S->n_iter += 1;
-    for (auto &f : failed) finish(S, f.first, RQ_FAILED, f.second);
-    S->active = todo;
-    if (st != GD_OK) {
-      for (Req *r : S->active) finish(S, r, RQ_FAILED, st);
-      S->active.clear();
-    } else {
-      for (Req *r : finished) {
-        finish(S, r, RQ_DONE, GD_OK);
-        S->active.erase(std::find(S->active.begin(), S->active.end(), r));
+    // cancelled members leave while their lane is idle
+    std::vector<Req *> cancelled;
+    {
+      std::lock_guard<std::mutex> g(S->mu);
+      for (auto &kv : S->lanes) {
+        Lane &L = *kv.second;
+        if (L.busy) continue;
+        std::vector<Req *> keep;
+        for (Req *r : L.members) (r->cancel ? cancelled : keep).push_back(r);
+        L.members.swap(keep);
       }
     }
-    if (!failed.empty() || !finished.empty() || st != GD_OK) S->done_cv.notify_all();
+    // relaunch every idle lane
+    for (auto &kv : S->lanes) {
+      Lane &L = *kv.second;
+      if (L.busy || (L.members.empty() && L.fresh.empty())) continue;
+      gd_status st = GD_OK;
+      if (!L.fresh.empty()) {
+        st = launch_lane(S, L, L.fresh, KMODE_INIT);
+        for (Req *r : L.fresh) L.members.push_back(r);
+        L.fresh.clear();
+      }
+      if (st == GD_OK) {
+        plan_steps(S, L.members);
+        st = launch_lane(S, L, L.members, KMODE_REMC);
+      }
+      if (st == GD_OK && cudaMemcpyAsync(L.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                         L.stream) != cudaSuccess)
+        st = fail(GD_ECUDA, "server: error word copy");
+      if (st == GD_OK && cudaEventRecord(L.done, L.stream) != cudaSuccess)
+        st = fail(GD_ECUDA, "server: event record");
+      if (st != GD_OK) {
+        cudaStreamSynchronize(L.stream);
+        for (Req *r : L.members) lane_failed.emplace_back(r, st);
+        L.members.clear();
+        continue;
+      }
+      L.in_flight = L.members;
+      L.busy = true;
+      S->n_iter += 1;
+      progressed = true;
+    }
+    {
+      std::lock_guard<std::mutex> g(S->mu);
+      for (auto &f : failed) finish(S, f.first, RQ_FAILED, f.second);
+      for (auto &f : lane_failed) finish(S, f.first, RQ_FAILED, f.second);
+      for (Req *r : cancelled) finish(S, r, RQ_CANCELLED, GD_ECANCELLED);
+      for (Req *r : finished) finish(S, r, RQ_DONE, GD_OK);
+      if (!failed.empty() || !lane_failed.empty() || !cancelled.empty() || !finished.empty())
+        S->done_cv.notify_all();
+    }
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(100));
   }
+  // stopping: wait for the lanes' launches to end
+  for (auto &kv : S->lanes)
+    if (kv.second->busy) cudaEventSynchronize(kv.second->done);
 }
 
 gd_status copy_request(gd_server *S, int protein_id, const gd_complex *cx,
@@ -537,7 +635,15 @@ extern "C" gd_status gd_server_create(int device, size_t hbm_budget_bytes, int m
   S->budget = hbm_budget_bytes;
   S->max_active = max_active > 0 ? max_active : 2 * ctx->n_sm;
   S->steps_per_launch = steps_per_launch;
-  cudaEventCreateWithFlags(&S->ev, cudaEventBlockingSync);
+  if (cudaMalloc(&S->d_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess ||
+      cudaMemset(S->d_err_pool, 0, kMaxLanes * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&S->h_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess) {
+    if (S->d_err_pool) cudaFree(S->d_err_pool);
+    ctx_release(ctx);
+    delete S;
+    return fail(GD_ENOMEM, "server error words");
+  }
+  std::memset(S->h_err_pool, 0, kMaxLanes * sizeof(int));
   S->th = std::thread(scheduler, S);
   *out = S;
   return GD_OK;
@@ -709,13 +815,21 @@ extern "C" gd_status gd_server_destroy(gd_server *S) {
   }
   if (S->th.joinable()) S->th.join();
   cudaSetDevice(S->ctx->device);
-  for (Req *r : S->active) release_device(S, r);
+  for (Req *r : S->active)
+    if (r->stream) release_device(r);
   cudaStreamSynchronize(S->ctx->stream);
   for (auto &p : S->proteins) dcx_release(p->dcx);
-  if (S->d_items) cudaFree(S->d_items);
-  if (S->d_cta) cudaFree(S->d_cta);
-  if (S->d_groups) cudaFree(S->d_groups);
-  if (S->ev) cudaEventDestroy(S->ev);
+  for (auto &kv : S->lanes) {
+    Lane &L = *kv.second;
+    cudaStreamSynchronize(L.stream);
+    if (L.d_items) cudaFree(L.d_items);
+    if (L.d_cta) cudaFree(L.d_cta);
+    if (L.d_groups) cudaFree(L.d_groups);
+    cudaEventDestroy(L.done);
+    cudaStreamDestroy(L.stream);
+  }
+  if (S->d_err_pool) cudaFree(S->d_err_pool);
+  if (S->h_err_pool) cudaFreeHost(S->h_err_pool);
   ctx_release(S->ctx);
   delete S;
   return GD_OK;
