@@ -162,6 +162,13 @@ void dcx_release(gd_dcomplex *d) {
   ctx_release(c);
 }
 
+gd_status kernel_error(int code) {
+  if (code == 3)
+    return fail(GD_ECUDA, "internal: a warp needs more H-bond atom pairs than its launch "
+                          "shape evaluates");
+  return fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)", code);
+}
+
 gd_status ctx_check(gd_ctx *c) {
   int h = 0;
   GD_CUDA(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -169,7 +176,7 @@ gd_status ctx_check(gd_ctx *c) {
   if (h != 0) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
     cudaStreamSynchronize(c->stream);
-    return fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)", h);
+    return kernel_error(h);
   }
   return GD_OK;
 }
@@ -516,11 +523,13 @@ static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
   // kernel slot order: atoms with an H-bond term (some point type with
   // hdb0 > 0.1) first, so that they share atom pairs and warps
   std::vector<int> order;
+  T.n_hb = 0;
   for (int pass = 0; pass < 2; ++pass)
     for (int a = 0; a < lna; ++a) {
       bool hb = false;
       for (int j = 0; j < GD_NPT; ++j) hb = hb || F.hdb0[L.t[a]][j] > 0.1f;
       if (hb == (pass == 0)) order.push_back(a);
+      if (hb && pass == 0) ++T.n_hb;
     }
   GD_TRY(upload(d, order, &T.lig_order));
   for (int i = 0; i < GD_NLT; ++i) {
@@ -664,6 +673,7 @@ static gd_status poses_launch(gd_ctx *ctx, const gd_dcomplex *d, const Tile &til
   R.terms = terms;
   R.raw = raw;
   R.err = ctx->d_err;
+  R.hb_pairs = hb_pairs_of(d->T, tile.A);
   KItem it{};
   it.T = d->T;
   it.n_tmp = 1;

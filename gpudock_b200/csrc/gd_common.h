@@ -90,6 +90,8 @@ void ctx_release(gd_ctx *c);
 void dcx_retain(gd_dcomplex *d);
 void dcx_release(gd_dcomplex *d);
 gd_status ctx_check(gd_ctx *c);
+// Status for a nonzero kernel error word (KRun.err).
+gd_status kernel_error(int code);
 // Ligand-size bucket: sizes are rounded up to a multiple of 8 atoms; launch
 // shapes are chosen (and autotuned) per bucket and cover its largest size.
 int lna_bucket(int lna);

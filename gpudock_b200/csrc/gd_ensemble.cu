@@ -35,6 +35,7 @@ struct Plan {
   Tile tile;
   double cost = 0.0;  // sum over its CTAs of ligand atoms x protein points
   int n_stages = 0, resident = 0, group_major = 0, fused = 0, grid = 0;
+  int hb_pairs = 0;  // largest hb_pairs_of over its items
   int *d_cta_item = nullptr, *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
 };
 
@@ -206,6 +207,7 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
     pl.resident = res;
     pl.group_major = gm ? 1 : 0;
     pl.fused = gm ? 1 : 0;
+    pl.hb_pairs = std::max(pl.hb_pairs, hb_pairs_of(I.T, t.A));
     const double cost = (double)I.T.lna * I.T.pnp;
     auto &list = ctas[key];
     if (gm) {
@@ -276,6 +278,7 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   R.fused_exchange = pl.fused;
   R.spe = E.spe;
   R.err = E.ctx->d_err;
+  R.hb_pairs = pl.hb_pairs;
   return R;
 }
 

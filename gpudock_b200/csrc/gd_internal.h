@@ -59,7 +59,9 @@ struct KTables {
   const float *mcs_cnt; // [pos] number of valid atoms (float)
   const uint32_t *mcc_ref;  // [lna][mcc_words] reference contact map (bits)
   int lna, n_lig, pnp, pnp_pad, n_prt, pos, psp_ncol, mcc_words;
-  float mcc_nref;       // contacts in the reference map
+  int n_hb;             // atoms with an H-bond term (the first n_hb slots)
+  int pad1;
+  float mcc_nref;      // contacts in the reference map
   float near_mcc2;      // squared distance within which a contact can occur
                         // (max pmf0^2, with margin)
   float near_ele2;      // squared distance of the near-field electrostatics
@@ -125,8 +127,17 @@ struct KRun {
   int step0, n_steps;
   const int *step_ptr;
   int item_step;
-  int *err;              // error word (bounded waits)
+  int hb_pairs;          // most atom pairs with an H-bond term in any warp of
+                         // any item (hb_pairs_of); selects the kernel variant
+  int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too low
 };
+
+// Atom pairs of warp 0 (the most) holding a slot below n_hb: a warp's pair h
+// holds slots ag + 2hA and ag + (2h+1)A.
+inline int hb_pairs_of(const KTables &T, int A) {
+  const int k = (T.n_hb + A - 1) / A;
+  return (k + 1) / 2;
+}
 
 // Exchange groups: one (item, protein conf, ligand conf) each.
 struct KGroup {

@@ -345,9 +345,9 @@ struct PairConst {
 // LJ and PMF quotients share one reciprocal: with D1 = p4 and
 // D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the point
 // type's entry of atom pair 0 of this warp's pair tables.
-template <bool HDB>
-__device__ __forceinline__ void pair_hh(float2 nx, float2 ny, float2 nz, const float4 &Ap,
-                                        const float4 *pp, const float4 *hp, int h,
+__device__ __forceinline__ void pair_hh(const bool hdb, float2 nx, float2 ny, float2 nz,
+                                        const float4 &Ap, const float4 *pp, const float4 *hp,
+                                        int h,
                                         const PairConst &K, float2 &fvdw, float2 &fpmf,
                                         float2 &fhdb, float2 &fek, float &mn) {
   const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
@@ -374,7 +374,7 @@ __device__ __forceinline__ void pair_hh(float2 nx, float2 ny, float2 nz, const f
   fpmf = fma2(mul2(hi2(T1), p4), inv, fpmf);
   fek = fma2(dup2(Ap.w), r, fek);
   mn = fminf(mn, fminf(d2.x, d2.y));
-  if (HDB) {
+  if (hdb) {  // a compile-time constant at every (inlined, unrolled) call
     // weight 0 (and h3 = 0) for the atoms of the pair without the term
     const float4 H = hp[h * PT_ROWS];  // -hdb0, w
     const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
@@ -383,24 +383,26 @@ __device__ __forceinline__ void pair_hh(float2 nx, float2 ny, float2 nz, const f
   }
 }
 
-// One protein point against this lane's NA atoms (branch-free body).
-template <int NH, bool HDB>
+// One protein point against this lane's NA atoms (branch-free body).  The
+// H-bond term runs for the first NHB atom pairs only: H-bond-capable atoms
+// come first in the slot order, so the later pairs of a warp have none.
+template <int NH, int NHB>
 __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                             const float2 (&nz)[NH], const float4 &A0,
                                             const float4 *pp, const float4 *hp,
                                             const PairConst &K, float2 &fvdw, float2 &fpmf,
                                             float2 &fhdb, float2 (&fek)[NH], float &mn) {
 #pragma unroll
-  for (int h = 0; h < NH; ++h)
-    pair_hh<HDB>(nx[h], ny[h], nz[h], A0, pp, hp, h, K, fvdw, fpmf, fhdb, fek[h], mn);
+  for (int h = 0; h < NH; ++h)  // unrolled: h < NHB folds to a constant
+    pair_hh(h < NHB, nx[h], ny[h], nz[h], A0, pp, hp, h, K, fvdw, fpmf, fhdb, fek[h], mn);
 }
 
 // The fast path over points j0 .. j1-1 of a staged tile, one point per
 // iteration and no branch in the body, so the compiler can overlap one
 // point's tail with the next point's head.  Returns the mask of points whose
 // close-range terms must run: some lane has an atom within the point's
-// threshold (thr_l, held by lane j - j0).
-template <int NH, bool HDB>
+// threshold (thr_l, held by lane j - j0).  NHB: atom pairs with the H-bond term.
+template <int NH, int NHB>
 __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                                const float2 (&nz)[NH], const float4 *ta,
                                                const float2 *tb, int j0, int j1,
@@ -413,7 +415,7 @@ __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const flo
     const float4 Ap = ta[j];
     const int pt = (int)(__float_as_uint(tb[j].y) & META_TYPE_MASK);
     float mn = 3.0e38f;
-    pair_block1<NH, HDB>(nx, ny, nz, Ap, my_ptab + pt * 2, my_htab + pt, K, fvdw, fpmf, fhdb,
+    pair_block1<NH, NHB>(nx, ny, nz, Ap, my_ptab + pt * 2, my_htab + pt, K, fvdw, fpmf, fhdb,
                          fek, mn);
     const float thr = __shfl_sync(0xffffffffu, thr_l, j - j0);
     close |= (__any_sync(0xffffffffu, mn <= thr) ? 1u : 0u) << (j - j0);
@@ -478,14 +480,17 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
   }
 }
 
-template <int MODE, int NA>
+// HB: atom pairs per warp that evaluate the H-bond term (at least what the
+// launch's items need, KRun.hb_pairs).
 // No producer warp: sm_100 splits the register file between the four
 // schedulers, so a 13th warp would put four warps on one scheduler and cap
 // every thread at 128 registers; 12 warps leave room for about 168.
+template <int MODE, int NA, int HB>
 __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     dock_kernel(const __grid_constant__ KRun R) {
   static_assert(NA % 2 == 0, "atoms are processed in pairs");
   constexpr int NH = NA / 2;
+  static_assert(HB >= 0 && HB <= NH, "H-bond pair bound");
   extern __shared__ __align__(128) unsigned char smem[];
   const int A = R.A, P = R.P, W = A * P, NS = R.n_stages;
   const int MAXA = A * NA;
@@ -654,6 +659,12 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   const float4 *my_htab = s_htab + (size_t)ag * NH * PT_ROWS;
   const uint32_t *my_hmask = s_hmask + (size_t)ag * PT_ROWS;
   const bool mcc_on = MODE != KMODE_POSES && (I.flags & GD_MC_MCC) != 0u;
+  // atom pairs of this warp with an H-bond term for some point type: the
+  // first my_nhb pairs (capable atoms come first in the slot order)
+  const int my_nhb =
+      32 - __clz(__reduce_or_sync(0xffffffffu, lane < PT_ROWS ? my_hmask[lane] : 0u));
+  // the host's bound must cover this warp; report it if not (code 3)
+  if (my_nhb > HB && lane == 0) atomicExch(R.err, 3);
 
   int it = 0;  // streaming ring position
   for (int si = 0; si < n_steps; ++si) {
@@ -762,11 +773,14 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         float thr_l = T.near4[((meta_l & META_HPC_BIT) ? 1 : 0) |
                               ((((meta_l >> META_CLASS_SHIFT) & 3u) == 2u) ? 2 : 0)];
         if (mcc_on) thr_l = fmaxf(thr_l, T.near_mcc2);
+        // two variants per kernel (each is a long unrolled body: more of them
+        // cost more in instruction fetch than skipping H-bond work saves)
         const uint32_t close =
-            chunk_hdb ? chunk_fast<NH, true>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
-                                             thr_l, fvdw, fpmf, fhdb, fek)
-                      : chunk_fast<NH, false>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
-                                              thr_l, fvdw, fpmf, fhdb, fek);
+            (chunk_hdb && my_nhb > 0)
+                ? chunk_fast<NH, HB>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K, thr_l,
+                                     fvdw, fpmf, fhdb, fek)
+                : chunk_fast<NH, 0>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K, thr_l,
+                                    fvdw, fpmf, fhdb, fek);
         for (uint32_t m = close; m != 0u; m &= m - 1u) {
           const int j = j0 + __ffs(m) - 1;
           const uint32_t meta = __float_as_uint(tb[j].y);
@@ -980,15 +994,28 @@ __global__ void fma_peak_kernel(float *out, int iters) {
 }
 
 // ---------------------------------------------------------------------------
-template <int MODE, int NA>
-static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
+template <int MODE, int NA, int HB>
+static cudaError_t launch_nahb(const KRun &R, int grid, cudaStream_t s) {
   const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages);
   const int threads = R.A * R.P * 32;
-  cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA>,
+  cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA, HB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dock_kernel<MODE, NA><<<grid, threads, smem, s>>>(R);
+  dock_kernel<MODE, NA, HB><<<grid, threads, smem, s>>>(R);
   return cudaGetLastError();
+}
+
+// Three H-bond bounds per NA: at most two or three pairs (ligands where up
+// to about a third or half of the atoms have the term, the common cases), or
+// every pair.
+template <int MODE, int NA>
+static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
+  constexpr int NH = NA / 2;
+  constexpr int HB2 = NH < 2 ? NH : 2;
+  constexpr int HB3 = NH < 3 ? NH : 3;
+  if (R.hb_pairs <= HB2) return launch_nahb<MODE, NA, HB2>(R, grid, s);
+  if (R.hb_pairs <= HB3) return launch_nahb<MODE, NA, HB3>(R, grid, s);
+  return launch_nahb<MODE, NA, NH>(R, grid, s);
 }
 
 template <int MODE>

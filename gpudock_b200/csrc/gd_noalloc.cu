@@ -96,6 +96,7 @@ extern "C" gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *d, 
   R.terms = d_terms;
   R.raw = raw ? d_raw : nullptr;
   R.err = ctx->d_err;
+  R.hb_pairs = gd::hb_pairs_of(d->T, tile.A);
   R.items = d_item;
   KItem it{};
   it.T = d->T;

@@ -341,6 +341,7 @@ gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int m
   R.n_steps = 0;  // per item (item_step)
   R.item_step = 1;
   R.err = L.d_err;
+  for (const Req *r : rs) R.hb_pairs = std::max(R.hb_pairs, hb_pairs_of(r->item.T, L.tile.A));
   GD_CUDA(launch_dock(R, L.tile.NA, (int)n_cta, s));
   S->ctx->launches += 1;
   S->n_launch += 1;
@@ -481,8 +482,7 @@ void scheduler(gd_server *S) {
         if (q != cudaSuccess) {
           st = fail(GD_ECUDA, "server launch: %s", cudaGetErrorString(q));
         } else if (*L.h_err != 0) {
-          st = fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)",
-                    *L.h_err);
+          st = kernel_error(*L.h_err);
           *L.h_err = 0;
           cudaMemsetAsync(L.d_err, 0, sizeof(int), L.stream);
         }

@@ -63,6 +63,38 @@ def test_batch_equals_alone(ctx, n_tmp):
         assert got.ac_mc == alone.ac_mc and got.ac_temp_exchg == alone.ac_temp_exchg
 
 
+def test_batch_hbond_mix_equals_alone(ctx):
+    """A ligand with an H-bond term on every atom and one with none share a
+    launch (same size bucket): the launch evaluates the term for every atom
+    pair, the term-free ligand alone skips it; trajectories stay identical."""
+    from tests.test_gpu_energy import hbond_types, with_ligand_types
+    pspec = synth.ComplexSpec(pnp=900, lna=8, n_prt=1)
+    cxs = _ligand_set(pspec, [40, 40], seed=44)
+    cap, free = hbond_types(cxs[0])
+    with_ligand_types(cxs[0], cap)
+    with_ligand_types(cxs[1], free)
+    _, mb = lib.set_temperature(8, 0.004, 0.04)
+    base = lib.DeviceComplex(ctx, cxs[0])
+    dcxs = [base, lib.DeviceComplex(ctx, cxs[1], share=base)]
+    steps, spe = 30, 10
+    flags = abi.MC_EXCHANGE | abi.MC_MOVE_AWAY
+    params = [abi.mc_params(steps, spe, mb, seed=9, stream_id=i, flags=flags) for i in range(2)]
+    b = lib.Batch(ctx, dcxs, params)
+    b.init()
+    b.run(steps)
+    for i, d in enumerate(dcxs):
+        got = b.read(i)
+        r = lib.Remc(d, steps, spe, mb, seed=9, stream_id=i, flags=flags)
+        r.init()
+        r.run(steps)
+        alone = r.read()
+        assert np.array_equal(got.energy, alone.energy), i
+        assert np.array_equal(got.movematrix, alone.movematrix), i
+    # the normalised H-bond term is constant (a * 0 + b) without H-bond atoms
+    assert np.unique(b.read(1).energy[..., abi.E_HDB]).size == 1
+    assert np.unique(b.read(0).energy[..., abi.E_HDB]).size > 1
+
+
 def test_batch_replay_against_oracle(ctx):
     """Decisions of a batched complex replay bit-exactly on the oracle."""
     pspec = synth.ComplexSpec(pnp=600, lna=8, n_prt=1)

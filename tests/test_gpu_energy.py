@@ -60,6 +60,39 @@ def test_energy_ligand_sizes(ctx, lna):
     _compare(cx, terms, raw, poses)
 
 
+def hbond_types(cx):
+    """Ligand types with an H-bond term for some point type (hdb0 > 0.1), and the rest."""
+    hd = np.ctypeslib.as_array(cx.ff.hdb0)[:abi.NLT]
+    cap = (hd > 0.1).any(axis=1)
+    return np.nonzero(cap)[0].astype(np.int32), np.nonzero(~cap)[0].astype(np.int32)
+
+
+def with_ligand_types(cx, pick):
+    """The complex with its ligand types replaced by draws from `pick`."""
+    rng = np.random.default_rng(int(cx.lig_t.sum()))
+    cx.lig_t = rng.choice(pick, size=len(cx.lig_t)).astype(np.int32)
+    cx._struct = None
+    return cx
+
+
+@pytest.mark.parametrize("which", ["all", "none"])
+@pytest.mark.parametrize("lna", [16, 40, 80])
+def test_energy_hbond_atom_counts(ctx, which, lna):
+    """Every atom with an H-bond term (the launch evaluates it for every atom
+    pair) or none (only the term-free chunk body runs)."""
+    cx = synth.make_complex(synth.ComplexSpec(pnp=1100, lna=lna), seed=200 + lna)
+    cap, free = hbond_types(cx)
+    with_ligand_types(cx, cap if which == "all" else free)
+    d = lib.DeviceComplex(ctx, cx)
+    poses = synth.random_poses(np.random.default_rng(lna), 64, box=3.0)
+    terms, raw = d.energy_poses(poses)
+    _compare(cx, terms, raw, poses)
+    if which == "none":
+        assert np.all(raw[:, abi.E_HDB] == 0.0)
+    else:
+        assert np.any(raw[:, abi.E_HDB] != 0.0)
+
+
 def test_energy_conformations(ctx):
     cx = synth.make_complex(synth.ComplexSpec(pnp=900, lna=20, n_prt=3, n_lig=4), seed=13)
     d = lib.DeviceComplex(ctx, cx)
