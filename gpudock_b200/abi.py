@@ -23,6 +23,8 @@ MC_MOVE_AWAY = 0x2
 MC_RECORD = 0x4
 MC_MCC = 0x8
 CMCC_INVALID = 10000.0
+# launch schedules (gd_ctx_set_schedule)
+SCHED_AUTO, SCHED_WAVES, SCHED_PERSISTENT = 0, 1, 2
 
 STATUS = {
     0: "GD_OK", 1: "GD_EINVAL", 2: "GD_ENOMEM", 3: "GD_EBUDGET", 4: "GD_ECUDA",

@@ -166,6 +166,9 @@ gd_status kernel_error(int code) {
   if (code == 3)
     return fail(GD_ECUDA, "internal: a warp needs more H-bond atom pairs than its launch "
                           "shape evaluates");
+  if (code == 4)
+    return fail(GD_ETIMEDOUT, "a persistent CTA gave up waiting for the earlier MC steps of "
+                              "its unit (code 4)");
   return fail(GD_ETIMEDOUT, "a bounded barrier wait gave up in a kernel (code %d)", code);
 }
 
@@ -762,6 +765,91 @@ extern "C" gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_til
   ctx->tiles[{lna_bucket(lna), (pnp + TILE_PTS - 1) / TILE_PTS}] = t;
   return GD_OK;
 }
+
+extern "C" gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines) {
+  if (!ctx) return fail(GD_EINVAL, "gd_ctx_set_schedule: NULL context");
+  if (mode < GD_SCHED_AUTO || mode > GD_SCHED_PERSISTENT)
+    return fail(GD_EINVAL, "gd_ctx_set_schedule: unknown mode %d", mode);
+  if (machines < 0) return fail(GD_EINVAL, "gd_ctx_set_schedule: machines=%d", machines);
+  ctx->sched_mode = mode;
+  ctx->sched_machines = machines;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_schedule_pieces(const double *cost, const int *steps, int n_units,
+                                        int machines, int *pieces, int cap, int *piece_off,
+                                        int *n_used) {
+  if (n_units < 0 || machines < 1 || cap < 0 || !piece_off || !n_used ||
+      (n_units > 0 && (!cost || !steps || !pieces)))
+    return fail(GD_EINVAL, "gd_schedule_pieces: bad arguments");
+  std::vector<double> c(cost, cost + n_units);
+  std::vector<int> s(steps, steps + n_units);
+  for (int u = 0; u < n_units; ++u)
+    if (!(c[u] > 0.0) || s[u] < 0)
+      return fail(GD_EINVAL, "gd_schedule_pieces: unit %d has cost %g, %d steps", u, c[u], s[u]);
+  std::vector<int4> pc;
+  std::vector<int> off;
+  const int used = schedule_pieces(c, s, machines, &pc, &off);
+  if ((int)pc.size() > cap)
+    return fail(GD_EINVAL, "gd_schedule_pieces: %zu pieces exceed cap %d", pc.size(), cap);
+  for (size_t k = 0; k < pc.size(); ++k) {
+    pieces[4 * k] = pc[k].x;
+    pieces[4 * k + 1] = pc[k].y;
+    pieces[4 * k + 2] = pc[k].z;
+    pieces[4 * k + 3] = pc[k].w;
+  }
+  for (int m = 0; m <= used; ++m) piece_off[m] = off[m];
+  *n_used = used;
+  return GD_OK;
+}
+
+namespace gd {
+
+int schedule_pieces(const std::vector<double> &cost, const std::vector<int> &steps, int m,
+                    std::vector<int4> *pieces, std::vector<int> *piece_off) {
+  pieces->clear();
+  piece_off->assign(1, 0);
+  double total = 0.0, longest = 0.0;
+  for (size_t u = 0; u < cost.size(); ++u) {
+    const double p = cost[u] * std::max(steps[u], 0);
+    total += p;
+    longest = std::max(longest, p);
+  }
+  if (total <= 0.0 || m < 1) return 0;
+  const double C = std::max(longest, total / m);
+  // line order: machine k holds [k C, (k+1) C) of the units laid end to end
+  std::vector<std::vector<int4>> mach(1);
+  double pos = 0.0;  // line length placed so far (cuts are rounded against
+                     // the ideal boundaries, so rounding does not accumulate)
+  for (size_t u = 0; u < cost.size(); ++u) {
+    const int n = steps[u];
+    const double c = cost[u];
+    int lo = 0;
+    while (lo < n) {
+      const double end = C * (double)mach.size();  // this machine's boundary
+      int s = (int)std::floor((end - pos) / c + 0.5);  // steps that fit, rounded
+      if (s >= n - lo || (int)mach.size() == m) s = n - lo;
+      if (s <= 0) {  // the machine is full: the unit starts the next one
+        mach.emplace_back();
+        continue;
+      }
+      mach.back().push_back(make_int4((int)u, lo, lo + s, lo > 0 ? 1 : 0));
+      lo += s;
+      pos += s * c;
+      if (lo < n) mach.emplace_back();  // cut: the rest opens the next machine
+    }
+  }
+  while (!mach.empty() && mach.back().empty()) mach.pop_back();
+  // run order is the reverse of line order: a cut unit's first steps open
+  // the lower machine, its last steps close the next one
+  for (auto &v : mach) {
+    for (auto p = v.rbegin(); p != v.rend(); ++p) pieces->push_back(*p);
+    piece_off->push_back((int)pieces->size());
+  }
+  return (int)mach.size();
+}
+
+}  // namespace gd
 
 // ---------------------------------------------------------------------------
 // Building blocks for tests

@@ -62,6 +62,8 @@ struct gd_ctx {
   int *d_err = nullptr;
   uint64_t launches = 0;
   int n_sm = 148;
+  int sched_mode = 0;      // GD_SCHED_*
+  int sched_machines = 0;  // persistent CTAs (0: SMs x occupancy)
   std::atomic<int> refs{1};
   // autotuned launch shapes keyed by (ligand-size bucket, protein tiles)
   std::mutex tile_mu;

@@ -165,4 +165,28 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Release store / acquire load of a word at GPU scope (progress flags
+// between CTAs of one launch).
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until *p >= target, for at most `limit` polls about 256 ns apart
+// (about four seconds by default); if it gives up it records `code` in *err
+// and returns false, so a lost flag costs a wrong result, not a hung GPU.
+__device__ __forceinline__ bool wait_progress(const int *p, int target, int *err, int code,
+                                              uint32_t limit = (1u << 24)) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (ld_acquire(p) >= target) return true;
+    __nanosleep(256);
+  }
+  if (err) atomicExch(err, code);
+  return false;
+}
+
 }  // namespace gd

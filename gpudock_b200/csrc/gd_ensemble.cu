@@ -37,6 +37,16 @@ struct Plan {
   int n_stages = 0, resident = 0, group_major = 0, fused = 0, grid = 0;
   int hb_pairs = 0;  // largest hb_pairs_of over its items
   int *d_cta_item = nullptr, *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
+  // persistent schedules (KRun.pieces) of this plan's units, by launch length
+  std::vector<double> unit_cost;  // [grid] cost of one MC step of each unit
+  int *d_progress = nullptr;      // [grid] MC steps done by each unit
+  int auto_machines = 0;          // SMs x resident CTAs per SM (0: not asked yet)
+  struct Sched {
+    int n_steps = 0, machines = 0, grid = 0;
+    int4 *d_pieces = nullptr;
+    int *d_off = nullptr, *d_ticket = nullptr;
+  };
+  std::vector<Sched> scheds;
 };
 
 struct Ens {
@@ -238,11 +248,13 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
       c0.push_back(std::get<2>(c));
       cn.push_back(std::get<3>(c));
       pl.cost += std::get<0>(c);
+      pl.unit_cost.push_back(std::get<0>(c));
     }
     pl.grid = (int)ci.size();
     GD_TRY(dcopy(E, &pl.d_cta_item, ci));
     GD_TRY(dcopy(E, &pl.d_cta_rep0, c0));
     GD_TRY(dcopy(E, &pl.d_cta_nrep, cn));
+    GD_TRY(dalloc(E, &pl.d_progress, ci.size()));
     E.plans.push_back(pl);
   }
   // costliest plans are issued first, so they start first on the SMs
@@ -282,6 +294,50 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   return R;
 }
 
+// Makes (once per launch length) the persistent schedule of every plan that
+// the context's schedule mode gives one; called outside stream capture.
+gd_status ens_prepare(Ens &E, int n_steps) {
+  const int mode = E.ctx->sched_mode;
+  if (mode == GD_SCHED_WAVES || n_steps < 2) return GD_OK;
+  for (Plan &pl : E.plans) {
+    if (pl.auto_machines == 0) {
+      KRun R = run_desc(E, pl, KMODE_REMC);
+      int occ = 0;
+      GD_CUDA(dock_ctas_per_sm(R, pl.tile.NA, &occ));
+      pl.auto_machines = std::max(1, occ) * E.ctx->n_sm;
+    }
+    const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
+    if (mode == GD_SCHED_AUTO && pl.grid <= machines) continue;
+    bool have = false;
+    for (const Plan::Sched &s : pl.scheds)
+      have = have || (s.n_steps == n_steps && s.machines == machines);
+    if (have) continue;
+    Plan::Sched s;
+    s.n_steps = n_steps;
+    s.machines = machines;
+    std::vector<int4> pieces;
+    std::vector<int> off;
+    s.grid = schedule_pieces(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines, &pieces,
+                             &off);
+    GD_TRY(dcopy(E, &s.d_pieces, pieces));
+    GD_TRY(dcopy(E, &s.d_off, off));
+    GD_TRY(dalloc(E, &s.d_ticket, 1));
+    pl.scheds.push_back(s);
+  }
+  return GD_OK;
+}
+
+// The schedule ens_prepare made for this plan and launch length, if any.
+const Plan::Sched *find_sched(const Ens &E, const Plan &pl, int n_steps) {
+  const int mode = E.ctx->sched_mode;
+  if (mode == GD_SCHED_WAVES) return nullptr;
+  const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
+  if (mode == GD_SCHED_AUTO && pl.grid <= machines) return nullptr;
+  for (const Plan::Sched &s : pl.scheds)
+    if (s.n_steps == n_steps && s.machines == machines) return &s;
+  return nullptr;
+}
+
 gd_status mark(Ens &E, int kind) {
   cudaEvent_t e;
   GD_CUDA(cudaEventCreate(&e));
@@ -304,7 +360,17 @@ gd_status launch_plans(Ens &E, int mode, int step0, int n_steps, bool device_ste
     R.step0 = step0;
     R.n_steps = n_steps;
     R.step_ptr = device_step ? E.d_step : nullptr;
-    GD_CUDA(launch_dock(R, pl.tile.NA, pl.grid, ss[k % n]));
+    int grid = pl.grid;
+    if (mode == KMODE_REMC) {
+      if (const Plan::Sched *sc = find_sched(E, pl, n_steps)) {
+        R.pieces = sc->d_pieces;
+        R.piece_off = sc->d_off;
+        R.ticket = sc->d_ticket;
+        R.progress = pl.d_progress;
+        grid = sc->grid;
+      }
+    }
+    GD_CUDA(launch_dock(R, pl.tile.NA, grid, ss[k % n]));
     E.ctx->launches += 1;
   }
   GD_TRY(join_streams(E.ctx, n));
@@ -317,6 +383,8 @@ gd_status ens_init(Ens &E) {
   cudaStream_t s = E.ctx->stream;
   GD_CUDA(cudaMemsetAsync(E.acs_exchg, 0, sizeof(int) * MAX_TMP * E.items.size(), s));
   GD_CUDA(cudaMemsetAsync(E.d_step, 0, sizeof(int), s));
+  for (const Plan &pl : E.plans)  // progress counts steps from 0 again
+    GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
   GD_TRY(launch_plans(E, KMODE_INIT, 0, 1, false));
   E.step = 0;
   E.t_compute = 0.0;
@@ -360,6 +428,9 @@ gd_status ens_run(Ens &E, int n_steps) {
   if (n_steps == 0) return GD_OK;
   GD_CUDA(cudaSetDevice(E.ctx->device));
   cudaStream_t s = E.ctx->stream;
+  // launch length: the whole run when the exchange is inside the kernel,
+  // else one interval (per launch, or in the captured graph)
+  GD_TRY(ens_prepare(E, E.all_fused ? n_steps : E.spe));
   GD_CUDA(cudaEventRecord(E.ev0, s));
   // keep the device step counter in step with the host's
   GD_CUDA(cudaMemcpyAsync(E.d_step, &E.step, sizeof(int), cudaMemcpyHostToDevice, s));

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/gpudock.h"
@@ -129,8 +130,31 @@ struct KRun {
   int item_step;
   int hb_pairs;          // most atom pairs with an H-bond term in any warp of
                          // any item (hb_pairs_of); selects the kernel variant
-  int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too low
+  // Persistent schedule (REMC; nullptr: CTA b runs every step of unit b,
+  // where a unit is one entry of cta_item / cta_rep0 / cta_nrep).  CTA m, in
+  // the order the CTAs start, runs pieces piece_off[m] .. piece_off[m+1]-1,
+  // each {unit, first step, end step, wait}: MC steps [first, end) of the
+  // launch for that unit, after waiting (wait != 0) until progress[unit]
+  // reaches the launch's first step + first.
+  const int4 *pieces;
+  const int *piece_off;  // [grid + 1]
+  int *ticket;           // start-order counter, 0 before the launch (wraps)
+  int *progress;         // [units] MC steps done (absolute step count)
+  int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too
+                         // low, 4 a piece's predecessor never finished
 };
+
+// McNaughton's wrap-around rule, for MC steps that must run in order: units
+// of `cost[u]` per step and `steps[u]` steps each are laid end to end and cut
+// into `m` machines of equal length C = max(max_u cost[u] steps[u],
+// sum / m), each cut at a step boundary.  A unit cut at a machine boundary
+// runs its first steps at the start of the lower machine and the rest at the
+// end of the next one (after a wait that therefore rarely blocks), so each
+// machine waits only on the one before it.  Returns the pieces grouped by
+// machine (piece_off[m] .. piece_off[m+1]-1, in run order) and the number of
+// machines that got work.
+int schedule_pieces(const std::vector<double> &cost, const std::vector<int> &steps, int m,
+                    std::vector<int4> *pieces, std::vector<int> *piece_off);
 
 // Atom pairs of warp 0 (the most) holding a slot below n_hb: a warp's pair h
 // holds slots ag + 2hA and ag + (2h+1)A.
@@ -148,6 +172,8 @@ size_t dock_smem_bytes(int A, int P, int NA, int n_stages);
 
 // Kernel launchers (gd_kernels.cu); return the launch status.
 cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s);
+// CTAs of the launch's kernel variant resident per SM (occupancy).
+cudaError_t dock_ctas_per_sm(const KRun &R, int NA, int *n);
 cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups, int spe,
                             int step0, const int *step_ptr, cudaStream_t s);
 cudaError_t launch_advance(int *step_ptr, int spe, cudaStream_t s);

@@ -77,13 +77,35 @@ static_assert(sizeof(KItem) % 8 == 0, "KItem must keep the barriers 8-byte align
 // hmask[ag][pt] has bit h set when pair h of group ag has an H-bond term with
 // point type pt.  Slot s = ag + A k holds ligand atom order[s].
 struct SmemLayout {
-  size_t ptab, htab, hmask, slot_q, slot_t, slot_a, tiles, red, hpc, lane, item, bars, total;
+  size_t ptab, htab, hmask, slot_q, slot_t, slot_a, tiles, red, hpc, lane, item, bars, ctl,
+      total;
 };
+
+// Piece bookkeeping of a CTA, in shared memory so that none of it holds a
+// register across the pair loop.  A piece is a range of MC steps of one
+// unit (a CTA's worth of replicas); without a schedule a CTA runs one piece,
+// all steps of unit blockIdx.x.
+struct PieceCtl {
+  int pc, pc_end;   // next piece, end of this CTA's pieces
+  int item;         // item whose tables are in shared memory (-1: none)
+  int tiles_key;    // item * MAX_PRT_KEY + protein conformation of the
+                    // resident tiles (-1: none)
+  int gen;          // resident tile loads so far (mbarrier phase parity)
+  int it;           // streaming ring position (continues across pieces)
+  int first_it;     // ring position of the current piece's first tile
+  int sig_unit;     // unit of the current piece, and the step count its
+  int sig_step;     // progress word holds once the piece has ended
+  int pad;
+};
+constexpr int MAX_PRT_KEY = 1 << 16;
+static_assert(sizeof(PieceCtl) <= 64, "PieceCtl fits its slot");
 
 __host__ __device__ inline SmemLayout smem_layout(int A, int P, int NA, int NS) {
   SmemLayout L;
   const size_t NH = NA / 2, MAXA = (size_t)A * NA, W = (size_t)A * P;
   size_t o = 0;
+  L.ctl = o;  // first, at a fixed address
+  o += 64;
   L.ptab = o;
   o += (size_t)A * NH * PT_ROWS * 32;
   L.htab = o;
@@ -481,11 +503,13 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
 }
 
 // HB: atom pairs per warp that evaluate the H-bond term (at least what the
-// launch's items need, KRun.hb_pairs).
+// launch's items need, KRun.hb_pairs).  PIECES: the CTA runs the pieces of a
+// persistent schedule (KRun.pieces, REMC only), else all steps of unit
+// blockIdx.x.
 // No producer warp: sm_100 splits the register file between the four
 // schedulers, so a 13th warp would put four warps on one scheduler and cap
 // every thread at 128 registers; 12 warps leave room for about 168.
-template <int MODE, int NA, int HB>
+template <int MODE, int NA, int HB, bool PIECES>
 __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     dock_kernel(const __grid_constant__ KRun R) {
   static_assert(NA % 2 == 0, "atoms are processed in pairs");
@@ -508,14 +532,53 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   KItem *s_item = reinterpret_cast<KItem *>(smem + SL.item);
   uint64_t *s_full = reinterpret_cast<uint64_t *>(smem + SL.bars);
   int *s_done = reinterpret_cast<int *>(s_full + NS);  // warps done with a stage
+  PieceCtl *s_ctl = reinterpret_cast<PieceCtl *>(smem);  // SmemLayout.ctl == 0
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
 
-  // ---- item of this CTA into shared memory, pair tables, barriers ---------
-  const int item = (MODE == KMODE_POSES) ? 0 : R.cta_item[blockIdx.x];
-  const KItem &G = R.items[item];
-  {
+  // ---- barriers and the pieces of this CTA ----------------------------------
+  // With a schedule (PIECES, R.pieces) a CTA's number is a ticket taken when it
+  // starts (wrapping back to 0 after the last CTA), so a CTA only ever waits
+  // on one that started before it.
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(&s_full[i], 1);
+      s_done[i] = 0;
+    }
+    fence_barrier_init();
+    int pc = 0, pc_end = 1;
+    if (PIECES) {
+      const int m = (int)atomicInc(reinterpret_cast<unsigned *>(R.ticket), gridDim.x - 1);
+      pc = R.piece_off[m];
+      pc_end = R.piece_off[m + 1];
+    }
+    s_ctl->pc = pc;
+    s_ctl->pc_end = pc_end;
+    s_ctl->item = -1;
+    s_ctl->tiles_key = -1;
+    s_ctl->gen = 0;
+    s_ctl->it = 0;
+  }
+  __syncthreads();
+
+  for (;;) {
+  const int pc = s_ctl->pc;
+  if (pc >= s_ctl->pc_end) break;
+  int unit = blockIdx.x, lo = 0, hi = -1;  // hi < 0: every step of the launch
+  bool wait_dep = false;
+  if (PIECES) {
+    const int4 pz = R.pieces[pc];
+    unit = pz.x;
+    lo = pz.y;
+    hi = pz.z;
+    wait_dep = pz.w != 0;
+  }
+
+  // ---- item of this piece into shared memory, pair tables -----------------
+  const int item = (MODE == KMODE_POSES) ? 0 : R.cta_item[unit];
+  if (item != s_ctl->item) {
+    const KItem &G = R.items[item];
     const uint32_t *src = reinterpret_cast<const uint32_t *>(&G);
     uint32_t *dst = reinterpret_cast<uint32_t *>(s_item);
     for (int i = threadIdx.x; i < (int)(sizeof(KItem) / 4); i += blockDim.x) dst[i] = src[i];
@@ -556,19 +619,13 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       }
       s_hmask[i] = m;
     }
+    __syncthreads();  // every thread has read s_ctl->item
+    if (threadIdx.x == 0) s_ctl->item = item;
   }
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < NS; ++i) {
-      mbar_init(&s_full[i], 1);
-      s_done[i] = 0;
-    }
-    fence_barrier_init();
-  }
-  __syncthreads();
   const KItem &I = *s_item;
   const KTables &T = I.T;
 
-  // ---- work of this CTA --------------------------------------------------
+  // ---- work of this piece ---------------------------------------------------
   int rep0, n_act, prt_conf, lane_rep;
   if (MODE == KMODE_POSES) {
     rep0 = blockIdx.x * 32;
@@ -578,42 +635,69 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   } else if (R.group_major) {
     // whole exchange groups: lane = group offset * n_tmp + temperature slot
     const int nt = I.n_tmp, nl = I.n_lig_conf;
-    const int g0 = R.cta_rep0[blockIdx.x];
-    n_act = R.cta_nrep[blockIdx.x];
+    const int g0 = R.cta_rep0[unit];
+    n_act = R.cta_nrep[unit];
     rep0 = g0;
     prt_conf = g0 / nl;
     const int ln = lane < n_act ? lane : 0;
     lane_rep = nt * nl * prt_conf + nl * (ln % nt) + (g0 % nl) + ln / nt;
   } else {
-    rep0 = R.cta_rep0[blockIdx.x];
-    n_act = R.cta_nrep[blockIdx.x];
+    rep0 = R.cta_rep0[unit];
+    n_act = R.cta_nrep[unit];
     prt_conf = rep0 / (I.n_tmp * I.n_lig_conf);
     lane_rep = rep0 + (lane < n_act ? lane : 0);
   }
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
   const bool resident = R.resident != 0;
-  const int n_steps = (MODE != KMODE_REMC) ? 1 : (R.item_step ? I.n_run : R.n_steps);
+  const int launch_steps = (MODE != KMODE_REMC) ? 1 : (R.item_step ? I.n_run : R.n_steps);
+  const int launch_base = (MODE == KMODE_REMC && R.item_step)  ? I.step0
+                          : (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr
+                                                               : R.step0;
+  // this piece: MC steps lo .. hi-1 of the launch
+  const int s_hi = hi < 0 ? launch_steps : hi;
+  const int n_steps = s_hi - lo;
+  const int step_base = launch_base + lo;
   const int passes = resident ? 1 : n_steps;
-  const int step_base = (MODE == KMODE_REMC && R.item_step)  ? I.step0
-                        : (MODE == KMODE_REMC && R.step_ptr) ? *R.step_ptr
-                                                             : R.step0;
 
-  // ---- protein staging: the tile sequence of the launch (every tile once
-  // when resident, else all tiles once per MC step through the NS-stage
-  // ring).  Thread 0 issues the first NS copies; afterwards the last warp to
-  // finish a stage (elected by the s_done counter) refills it.
+  // ---- protein staging: the tile sequence of the piece (every tile once
+  // when resident and not already in place, else all tiles once per MC step
+  // through the NS-stage ring).  Thread 0 issues the first copies; afterwards
+  // the last warp to finish a stage (elected by the s_done counter) refills it.
   const float4 *src_a = T.pt_a + (size_t)prt_conf * T.pnp_pad;
   const float2 *src_b = T.pt_b;
   const int n_seq = passes * n_tiles;
-  auto issue_tile = [&](int q) {
-    const int s = q % NS, t = q % n_tiles;
+  auto issue_tile = [&](int s, int t) {
     unsigned char *dst = s_tiles + (size_t)s * STAGE_BYTES;
     mbar_arrive_expect_tx(&s_full[s], STAGE_BYTES);
     bulk_g2s(dst, src_a + (size_t)t * TILE_PTS, TILE_PTS * 16, &s_full[s]);
     bulk_g2s(dst + TILE_PTS * 16, src_b + (size_t)t * TILE_PTS, TILE_PTS * 8, &s_full[s]);
   };
-  if (threadIdx.x == 0)
-    for (int q = 0; q < min(NS, n_seq); ++q) issue_tile(q);
+  int it = s_ctl->it;  // ring position of the piece's first tile
+  const int tiles_key = item * MAX_PRT_KEY + prt_conf;
+  const bool reload = resident && tiles_key != s_ctl->tiles_key;
+  const int gen = s_ctl->gen + (reload ? 1 : 0);
+  if (threadIdx.x == 0) {
+    // the previous piece's reads of the stages are ordered before the copies
+    // by the barrier that ended it
+    fence_proxy_async_smem();
+    if (resident) {
+      if (reload)
+        for (int t = 0; t < n_tiles; ++t) issue_tile(t, t);
+    } else {
+      for (int q = 0; q < min(NS, n_seq); ++q) issue_tile((it + q) % NS, q % n_tiles);
+    }
+    // the steps before this piece ran on another CTA: wait until it has
+    // written their state back (bounded; code 4 if it never does)
+    if (wait_dep) wait_progress(R.progress + unit, step_base, R.err, 4);
+    s_ctl->first_it = it;
+    s_ctl->sig_unit = unit;
+    s_ctl->sig_step = launch_base + s_hi;
+  }
+  __syncthreads();  // every thread has read s_ctl; the dependency is met
+  if (threadIdx.x == 0) {
+    s_ctl->tiles_key = resident ? tiles_key : -1;
+    s_ctl->gen = gen;
+  }
 
   // ---- compute warps -----------------------------------------------------
   const int ag = warp % A, pg = warp / A;
@@ -632,13 +716,15 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     me.idx_tmp = 0;
     me.mbeta = 0.f;
     if (MODE == KMODE_REMC) {
-      me.idx_tmp = I.idx_tmp[rep];
+      // through L2: the state may have been written by another CTA
+      me.idx_tmp = __ldcg(&I.idx_tmp[rep]);
       me.mbeta = I.minus_beta[me.idx_tmp];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) me.m_old[i] = I.m_old[(size_t)rep * 6 + i];
+      for (int i = 0; i < 6; ++i) me.m_old[i] = __ldcg(&I.m_old[(size_t)rep * 6 + i]);
 #pragma unroll
-      for (int i = 0; i < GD_NTERM; ++i) me.e_old[i] = I.e_old[(size_t)rep * GD_NTERM + i];
-      me.cmcc_old = I.cmcc ? I.cmcc[rep] : 0.f;
+      for (int i = 0; i < GD_NTERM; ++i)
+        me.e_old[i] = __ldcg(&I.e_old[(size_t)rep * GD_NTERM + i]);
+      me.cmcc_old = I.cmcc ? __ldcg(&I.cmcc[rep]) : 0.f;
     } else {
 #pragma unroll
       for (int i = 0; i < 6; ++i) me.m_old[i] = 0.f;
@@ -666,7 +752,6 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   // the host's bound must cover this warp; report it if not (code 3)
   if (my_nhb > HB && lane == 0) atomicExch(R.err, 3);
 
-  int it = 0;  // streaming ring position
   for (int si = 0; si < n_steps; ++si) {
     const int step = step_base + si;
 
@@ -750,7 +835,8 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       const int kstep = P;
       if (resident && k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile here
       const int s = resident ? t : (it % NS);
-      const uint32_t ph = resident ? 0u : (uint32_t)((it / NS) & 1);
+      // resident tiles: the phase of their latest load (s_ctl->gen loads so far)
+      const uint32_t ph = resident ? (uint32_t)((s_ctl->gen - 1) & 1) : (uint32_t)((it / NS) & 1);
       mbar_wait(&s_full[s], ph, R.err, 2);
       const float4 *ta = reinterpret_cast<const float4 *>(s_tiles + (size_t)s * STAGE_BYTES);
       const float2 *tb =
@@ -810,9 +896,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
           if (atomicAdd(&s_done[s], 1) == W - 1) {
             s_done[s] = 0;
             __threadfence_block();
-            if (it + NS < n_seq) {
+            const int q = it - s_ctl->first_it;  // position within the piece
+            if (q + NS < n_seq) {
               fence_proxy_async_smem();
-              issue_tile(it + NS);
+              issue_tile(s, (q + NS) % n_tiles);
             }
           }
         }
@@ -883,10 +970,24 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       I.acs_mc[rep] = 0;
       I.idx_tmp[rep] = (rep / I.n_lig_conf) % I.n_tmp;
     } else {
-      I.acs_mc[rep] += me.acs;
+      I.acs_mc[rep] = __ldcg(&I.acs_mc[rep]) + me.acs;
       if (R.fused_exchange) I.idx_tmp[rep] = me.idx_tmp;
     }
   }
+
+  // ---- end of the piece: publish its progress, move to the next ------------
+  // (without pieces the loop body runs once: no back edge, so the pair loop
+  // is compiled as in a plain kernel; a loop around it costs it registers)
+  if (!PIECES) break;
+  if (warp == 0) __threadfence();  // the state writes above, device-wide
+  __syncthreads();  // every warp is done with the stages, tables and lanes
+  if (threadIdx.x == 0) {
+    st_release(R.progress + s_ctl->sig_unit, s_ctl->sig_step);
+    s_ctl->pc += 1;
+    s_ctl->it = it;
+  }
+  __syncthreads();
+  }  // pieces
 }
 
 // Temperature exchange, one thread per (item, protein conf, ligand conf)
@@ -994,49 +1095,71 @@ __global__ void fma_peak_kernel(float *out, int iters) {
 }
 
 // ---------------------------------------------------------------------------
-template <int MODE, int NA, int HB>
-static cudaError_t launch_nahb(const KRun &R, int grid, cudaStream_t s) {
+template <int MODE, int NA, int HB, bool PIECES>
+static cudaError_t launch_kernel(const KRun &R, int grid, cudaStream_t s, int *occ) {
   const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages);
   const int threads = R.A * R.P * 32;
-  cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA, HB>,
+  cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA, HB, PIECES>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dock_kernel<MODE, NA, HB><<<grid, threads, smem, s>>>(R);
+  if (occ)  // occupancy query instead of a launch
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, dock_kernel<MODE, NA, HB, PIECES>,
+                                                         threads, smem);
+  dock_kernel<MODE, NA, HB, PIECES><<<grid, threads, smem, s>>>(R);
   return cudaGetLastError();
+}
+
+template <int MODE, int NA, int HB>
+static cudaError_t launch_nahb(const KRun &R, int grid, cudaStream_t s, int *occ) {
+  if constexpr (MODE == KMODE_REMC) {
+    if (R.pieces) return launch_kernel<MODE, NA, HB, true>(R, grid, s, occ);
+  } else {
+    if (R.pieces) return cudaErrorInvalidValue;  // schedules are for MC steps
+  }
+  return launch_kernel<MODE, NA, HB, false>(R, grid, s, occ);
 }
 
 // Three H-bond bounds per NA: at most two or three pairs (ligands where up
 // to about a third or half of the atoms have the term, the common cases), or
 // every pair.
 template <int MODE, int NA>
-static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s) {
+static cudaError_t launch_na(const KRun &R, int grid, cudaStream_t s, int *occ) {
   constexpr int NH = NA / 2;
   constexpr int HB2 = NH < 2 ? NH : 2;
   constexpr int HB3 = NH < 3 ? NH : 3;
-  if (R.hb_pairs <= HB2) return launch_nahb<MODE, NA, HB2>(R, grid, s);
-  if (R.hb_pairs <= HB3) return launch_nahb<MODE, NA, HB3>(R, grid, s);
-  return launch_nahb<MODE, NA, NH>(R, grid, s);
+  if (R.hb_pairs <= HB2) return launch_nahb<MODE, NA, HB2>(R, grid, s, occ);
+  if (R.hb_pairs <= HB3) return launch_nahb<MODE, NA, HB3>(R, grid, s, occ);
+  return launch_nahb<MODE, NA, NH>(R, grid, s, occ);
 }
 
 template <int MODE>
-static cudaError_t launch_mode(const KRun &R, int NA, int grid, cudaStream_t s) {
+static cudaError_t launch_mode(const KRun &R, int NA, int grid, cudaStream_t s, int *occ) {
   switch (NA) {
-    case 2: return launch_na<MODE, 2>(R, grid, s);
-    case 4: return launch_na<MODE, 4>(R, grid, s);
-    case 6: return launch_na<MODE, 6>(R, grid, s);
-    case 8: return launch_na<MODE, 8>(R, grid, s);
-    case 10: return launch_na<MODE, 10>(R, grid, s);
+    case 2: return launch_na<MODE, 2>(R, grid, s, occ);
+    case 4: return launch_na<MODE, 4>(R, grid, s, occ);
+    case 6: return launch_na<MODE, 6>(R, grid, s, occ);
+    case 8: return launch_na<MODE, 8>(R, grid, s, occ);
+    case 10: return launch_na<MODE, 10>(R, grid, s, occ);
     default: return cudaErrorInvalidValue;
+  }
+}
+
+static cudaError_t dock_dispatch(const KRun &R, int NA, int grid, cudaStream_t s, int *occ) {
+  switch (R.mode) {
+    case KMODE_POSES: return launch_mode<KMODE_POSES>(R, NA, grid, s, occ);
+    case KMODE_REMC: return launch_mode<KMODE_REMC>(R, NA, grid, s, occ);
+    default: return launch_mode<KMODE_INIT>(R, NA, grid, s, occ);
   }
 }
 
 cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
-  switch (R.mode) {
-    case KMODE_POSES: return launch_mode<KMODE_POSES>(R, NA, grid, s);
-    case KMODE_REMC: return launch_mode<KMODE_REMC>(R, NA, grid, s);
-    default: return launch_mode<KMODE_INIT>(R, NA, grid, s);
-  }
+  return dock_dispatch(R, NA, grid, s, nullptr);
+}
+
+cudaError_t dock_ctas_per_sm(const KRun &R, int NA, int *n) {
+  *n = 0;
+  return dock_dispatch(R, NA, 0, nullptr, n);
 }
 
 cudaError_t launch_exchange(const KItem *items, const KGroup *groups, int n_groups, int spe,

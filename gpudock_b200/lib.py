@@ -43,6 +43,10 @@ def _declare(lib):
                                      i32),
         "gd_autotune": ([P, P, C.POINTER(abi.GdTile), C.POINTER(C.c_double)], i32),
         "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
+        "gd_ctx_set_schedule": ([P, i32, i32], i32),
+        "gd_schedule_pieces": ([C.POINTER(C.c_double), C.POINTER(C.c_int), i32, i32,
+                                C.POINTER(C.c_int), i32, C.POINTER(C.c_int),
+                                C.POINTER(C.c_int)], i32),
         "gd_batch_create": ([P, i32, C.POINTER(P), C.POINTER(abi.GdMcParams), C.POINTER(P)], i32),
         "gd_batch_init": ([P], i32),
         "gd_batch_run": ([P, i32], i32),
@@ -152,6 +156,10 @@ class Context:
     @property
     def launches(self) -> int:
         return int(self._lib.gd_ctx_launch_count(self.h))
+
+    def set_schedule(self, mode: int, machines: int = 0):
+        """abi.SCHED_AUTO / SCHED_WAVES / SCHED_PERSISTENT (over `machines` CTAs)."""
+        check(self._lib.gd_ctx_set_schedule(self.h, mode, machines), "gd_ctx_set_schedule")
 
     def close(self):
         if self.h:
@@ -482,3 +490,25 @@ def fma_peak(ctx: Context, n_blocks: int = 148 * 16, iters: int = 4096):
     fl = C.c_double()
     check(ctx._lib.gd_fma_peak(ctx.h, n_blocks, iters, C.byref(ms), C.byref(fl)), "gd_fma_peak")
     return fl.value / (ms.value * 1e-3)
+
+
+def schedule_pieces(cost, steps, machines: int):
+    """The persistent schedule of units with per-step `cost` and `steps` MC
+    steps over `machines` CTAs: (pieces [n][4] = unit, first step, end step,
+    wait; piece_off [used + 1]), pieces of CTA m at piece_off[m]:piece_off[m+1]
+    in run order."""
+    lib = load()
+    cost = np.ascontiguousarray(cost, np.float64)
+    steps = np.ascontiguousarray(steps, np.int32)
+    n = len(cost)
+    cap = 2 * n + machines + 1
+    pieces = np.zeros((cap, 4), np.int32)
+    off = np.zeros(machines + 1, np.int32)
+    used = C.c_int(0)
+    check(lib.gd_schedule_pieces(cost.ctypes.data_as(C.POINTER(C.c_double)),
+                                 steps.ctypes.data_as(C.POINTER(C.c_int)), n, machines,
+                                 pieces.ctypes.data_as(C.POINTER(C.c_int)), cap,
+                                 off.ctypes.data_as(C.POINTER(C.c_int)), C.byref(used)),
+          "gd_schedule_pieces")
+    u = used.value
+    return pieces[:off[u]].copy(), off[:u + 1].copy()

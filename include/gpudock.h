@@ -252,6 +252,20 @@ gd_status gd_autotune(gd_ctx *ctx, const gd_dcomplex *dcx, gd_tile *best,
  * bucket of lna, i.e. lna rounded up to a multiple of 8). */
 gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile);
 
+/* How MC launches are spread over the SMs.  A unit is one CTA's worth of
+ * replicas (32 lanes).  GD_SCHED_AUTO (the default): a launch with more units
+ * than CTAs resident at once runs persistent CTAs, each taking a list of
+ * units and step ranges cut so that every CTA does the same amount of work
+ * (a unit may run its first steps on one CTA and the rest on another, after
+ * a bounded wait); otherwise one CTA per unit.  GD_SCHED_WAVES: always one
+ * CTA per unit.  GD_SCHED_PERSISTENT: always the persistent schedule, over
+ * `machines` CTAs (0: SMs x resident CTAs per SM).  Trajectories are
+ * bit-identical under every schedule.  Applies to launches enqueued after
+ * the call (a REMC run or batch keeps the schedule its captured graph was
+ * built with). */
+enum { GD_SCHED_AUTO = 0, GD_SCHED_WAVES = 1, GD_SCHED_PERSISTENT = 2 };
+gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
+
 /* ------------------------------------------------------------------------ */
 /* Pose energies (CalcEnergy_d after Move_d on a given move vector)         */
 /* ------------------------------------------------------------------------ */
@@ -468,6 +482,14 @@ gd_status gd_expf_dev(gd_ctx *ctx, int n, const float *x, float *y);
  * 8 chains x 16 FMAs x iters each; returns the time and the flop count. */
 gd_status gd_fma_peak(gd_ctx *ctx, int n_blocks, int iters, float *ms,
                       double *flops);
+/* The persistent schedule (host only, no device): n_units units of cost[u]
+ * per MC step and steps[u] steps over `machines` CTAs.  pieces[4 k ..] =
+ * {unit, first step, end step, wait} for k < piece_off[*n_used], CTA m's in
+ * piece_off[m] .. piece_off[m+1]-1 in run order; cap = room in pieces (in
+ * pieces of 4 ints), piece_off holds machines + 1 ints. */
+gd_status gd_schedule_pieces(const double *cost, const int *steps, int n_units,
+                             int machines, int *pieces, int cap, int *piece_off,
+                             int *n_used);
 
 #ifdef __cplusplus
 }
