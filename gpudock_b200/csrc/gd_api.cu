@@ -315,15 +315,18 @@ extern "C" gd_status gd_ctx_create(int device, void *stream, gd_ctx **out) {
     return fail(GD_ENODEV, "no CUDA device (%s)", cudaGetErrorString(e));
   if (device < 0 || device >= n) return fail(GD_EINVAL, "device %d of %d", device, n);
   GD_CUDA(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  GD_CUDA(cudaGetDeviceProperties(&prop, device));
-  if (prop.major != 10)
-    return fail(GD_ENODEV, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major,
-                prop.minor);
+  // single attributes (cudaGetDeviceProperties queries them all: slow)
+  int major = 0, minor = 0, n_sm = 0;
+  GD_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  GD_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+  GD_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+  if (major != 10)
+    return fail(GD_ENODEV, "device %d is sm_%d%d; this build targets sm_100a", device, major,
+                minor);
   gd_ctx *c = new (std::nothrow) gd_ctx;
   if (!c) return fail(GD_ENOMEM, "host allocation");
   c->device = device;
-  c->n_sm = prop.multiProcessorCount;
+  c->n_sm = n_sm;
   if (stream) {
     c->stream = (cudaStream_t)stream;
   } else {

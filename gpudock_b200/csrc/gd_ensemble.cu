@@ -73,10 +73,12 @@ struct Ens {
   std::vector<void *> allocs;
 };
 
+// Stream-ordered (cudaMallocAsync / cudaFreeAsync on the context stream):
+// creating and freeing a run never synchronises the device.
 template <typename T>
 gd_status dalloc(Ens &E, T **out, size_t n) {
   void *p = nullptr;
-  GD_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  GD_CUDA(cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), E.ctx->stream));
   E.allocs.push_back(p);
   GD_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), E.ctx->stream));
   *out = (T *)p;
@@ -115,7 +117,9 @@ void ens_free(Ens &E) {
   }
   if (E.gexec) cudaGraphExecDestroy(E.gexec);
   if (E.graph) cudaGraphDestroy(E.graph);
-  for (void *p : E.allocs) cudaFree(p);
+  if (E.ctx)
+    for (void *p : E.allocs) cudaFreeAsync(p, E.ctx->stream);
+  E.allocs.clear();
   for (cudaEvent_t e : E.prof_ev) cudaEventDestroy(e);
   if (E.ev0) cudaEventDestroy(E.ev0);
   if (E.ev1) cudaEventDestroy(E.ev1);
@@ -605,8 +609,12 @@ extern "C" gd_status gd_remc_kernel_times(gd_remc *r, double *mc_ms, int *mc_lau
 extern "C" gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log) {
   const auto t0 = std::chrono::steady_clock::now();
   GD_TRY(validate_mc(mc));
-  gd_ctx *ctx = nullptr;
-  GD_TRY(gd_ctx_create(0, nullptr, &ctx));
+  // one context per calling thread, kept between calls (its stream, side
+  // streams and launch-shape cache); everything of the run itself is
+  // stream-ordered and released at the end of the call
+  thread_local gd_ctx *ctx = nullptr;
+  if (!ctx) GD_TRY(gd_ctx_create(0, nullptr, &ctx));
+  GD_CUDA(cudaSetDevice(ctx->device));
   gd_dcomplex *d = nullptr;
   gd_remc *r = nullptr;
   gd_status st = gd_complex_upload(ctx, cx, &d);
@@ -616,7 +624,6 @@ extern "C" gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_
   if (st == GD_OK && log) st = gd_remc_read(r, log);
   gd_remc_destroy(r);
   gd_complex_free(d);
-  gd_ctx_destroy(ctx);
   if (st == GD_OK && log)
     log->t_wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return st;

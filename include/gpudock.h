@@ -393,7 +393,10 @@ gd_status gd_remc_kernel_times(gd_remc *remc, double *mc_ms, int *mc_launches,
                                double *exch_ms, int *exch_launches);
 
 /* One call with host buffers: upload, init, steps_total steps, read back,
- * free.  The counterpart of Run (run.cu:41-353). */
+ * free.  The counterpart of Run (run.cu:41-353).  Runs on device 0 through a
+ * context that each calling thread creates on its first call and keeps
+ * (stream, side streams, launch-shape cache); nothing of a run outlives the
+ * call. */
 gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc,
                  gd_mc_log *log);
 
