@@ -165,6 +165,24 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
                       f"{'-march=native' if native else 'x86-64'} OpenMP build)"}
 
 
+def profile_traffic(workload):
+    """DRAM bytes per launch of the headline kernel from the committed ncu
+    summary of this workload (dram__bytes_read.sum + dram__bytes_write.sum),
+    or None without one."""
+    import re
+    path = os.path.join(ROOT, "profiles", f"dock_kernel_remc_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    total = 0.0
+    for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+        m = re.search(r"`" + re.escape(key) + r"`\) \| ([0-9.]+) (\w+)", open(path).read())
+        if not m:
+            return None
+        total += float(m.group(1)) * scale.get(m.group(2), 1)
+    return total
+
+
 def _event_ms(stream, fn):
     import torch
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -522,7 +540,10 @@ def main():
                        "l2": "flushed (256 MiB write) before every step",
                        "parallelism": f"replicas, {ws} independent ensemble(s)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(w.name),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per "
+                                           "launch, ncu capture summarised in profiles/",
                          "kernel": "dock_kernel<REMC> (MC interval)",
                          "flops_per_launch": FLOP_PER_PAIR * pairs_per_launch,
                          "mean_launch_ms": mean_launch_s * 1e3, "launches": mc_n,
