@@ -29,10 +29,10 @@ SCHED_AUTO, SCHED_WAVES, SCHED_PERSISTENT = 0, 1, 2
 STATUS = {
     0: "GD_OK", 1: "GD_EINVAL", 2: "GD_ENOMEM", 3: "GD_EBUDGET", 4: "GD_ECUDA",
     5: "GD_ETIMEDOUT", 6: "GD_ECANCELLED", 7: "GD_ENOTFOUND", 8: "GD_EAGAIN",
-    9: "GD_ENODEV",
+    9: "GD_ENODEV", 10: "GD_EIO",
 }
 GD_OK, GD_EINVAL, GD_ENOMEM, GD_EBUDGET, GD_ECUDA = 0, 1, 2, 3, 4
-GD_ETIMEDOUT, GD_ECANCELLED, GD_ENOTFOUND, GD_EAGAIN, GD_ENODEV = 5, 6, 7, 8, 9
+GD_ETIMEDOUT, GD_ECANCELLED, GD_ENOTFOUND, GD_EAGAIN, GD_ENODEV, GD_EIO = 5, 6, 7, 8, 9, 10
 
 f32p = C.POINTER(C.c_float)
 i32p = C.POINTER(C.c_int)

@@ -17,9 +17,14 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <atomic>
+#include <cstddef>
+#include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <new>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -49,6 +54,30 @@ struct Plan {
   std::vector<Sched> scheds;
 };
 
+// Trajectory dumps of a run (gd_remc_set_trajectory): a two-dump device
+// ring the kernel writes records into, two pinned host slots, and a copy
+// stream on which each completed dump is copied and then written to disk by
+// a host function (so the compute stream never waits for the disk, only,
+// two dumps later, for the copy out of the ring half it is about to reuse).
+struct Traj {
+  std::string dir, stem;
+  int spd = 0;                 // MC steps per dump
+  int n_rep = 0;
+  int seq = 0;                 // number of the next file
+  gd_record *ring = nullptr;   // device [n_rep][2 spd]
+  gd_record *host[2] = {nullptr, nullptr};  // pinned [n_rep][spd]
+  cudaStream_t copy = nullptr;
+  cudaEvent_t done = nullptr;  // end of a dump on the compute stream
+  cudaEvent_t copied[2] = {nullptr, nullptr};
+  bool pending[2] = {false, false};  // copied[h] not yet waited on
+  std::atomic<int> err{0};     // a file could not be written
+};
+
+// LigRecordSingleStep (dock.h:487-493) is the first 88 bytes of gd_record.
+constexpr size_t kLigRecordBytes = 88;
+static_assert(offsetof(gd_record, e_prop_total) == kLigRecordBytes,
+              "gd_record must start with the LigRecordSingleStep fields");
+
 struct Ens {
   gd_ctx *ctx = nullptr;
   std::vector<gd_dcomplex *> dcx;
@@ -71,6 +100,7 @@ struct Ens {
   bool timing = false;
   double t_compute = 0.0;
   std::vector<void *> allocs;
+  std::unique_ptr<Traj> traj;
 };
 
 // Stream-ordered (cudaMallocAsync / cudaFreeAsync on the context stream):
@@ -114,6 +144,16 @@ void ens_free(Ens &E) {
   if (E.ctx) {
     cudaSetDevice(E.ctx->device);
     cudaStreamSynchronize(E.ctx->stream);
+  }
+  if (E.traj) {
+    Traj &t = *E.traj;
+    if (t.copy) cudaStreamSynchronize(t.copy);  // copies and file writes
+    for (cudaEvent_t e : {t.done, t.copied[0], t.copied[1]})
+      if (e) cudaEventDestroy(e);
+    if (t.copy) cudaStreamDestroy(t.copy);
+    for (gd_record *h : t.host)
+      if (h) cudaFreeHost(h);
+    E.traj.reset();
   }
   if (E.gexec) cudaGraphExecDestroy(E.gexec);
   if (E.graph) cudaGraphDestroy(E.graph);
@@ -392,6 +432,7 @@ gd_status ens_init(Ens &E) {
   GD_TRY(launch_plans(E, KMODE_INIT, 0, 1, false));
   E.step = 0;
   E.t_compute = 0.0;
+  if (E.traj) E.traj->seq = 0;  // a run's files are numbered from 0000
   return GD_OK;
 }
 
@@ -425,17 +466,12 @@ gd_status ens_enqueue(Ens &E, int n_steps, bool device_step) {
   return GD_OK;
 }
 
-gd_status ens_run(Ens &E, int n_steps) {
-  if (n_steps < 0 || n_steps % E.spe != 0)
-    return fail(GD_EINVAL, "n_steps %d is not a multiple of steps_per_exchange %d", n_steps,
-                E.spe);
-  if (n_steps == 0) return GD_OK;
-  GD_CUDA(cudaSetDevice(E.ctx->device));
+// n_steps (a multiple of spe) MC steps of every replica, enqueued.
+gd_status ens_run_steps(Ens &E, int n_steps) {
   cudaStream_t s = E.ctx->stream;
   // launch length: the whole run when the exchange is inside the kernel,
   // else one interval (per launch, or in the captured graph)
   GD_TRY(ens_prepare(E, E.all_fused ? n_steps : E.spe));
-  GD_CUDA(cudaEventRecord(E.ev0, s));
   // keep the device step counter in step with the host's
   GD_CUDA(cudaMemcpyAsync(E.d_step, &E.step, sizeof(int), cudaMemcpyHostToDevice, s));
   if (E.all_fused || E.profile) {
@@ -466,9 +502,163 @@ gd_status ens_run(Ens &E, int n_steps) {
       E.ctx->launches += per_graph;
     }
   }
+  E.step += n_steps;
+  return GD_OK;
+}
+
+// Writes the file of a dump after its records are copied out of ring half h.
+void CUDART_CB write_dump(void *arg);
+
+struct DumpJob {
+  Traj *t;
+  int slot, seq;
+};
+
+void CUDART_CB write_dump(void *arg) {
+  DumpJob *j = static_cast<DumpJob *>(arg);
+  Traj &t = *j->t;
+  char num[16];
+  std::snprintf(num, sizeof num, "%04d", j->seq);
+  const std::string path = t.dir + "/" + t.stem + "_" + num + ".bin";
+  FILE *f = std::fopen(path.c_str(), "wb");
+  bool ok = f != nullptr;
+  // pack the records to their 88-byte LigRecordSingleStep form in chunks
+  const gd_record *r = t.host[j->slot];
+  const size_t n = (size_t)t.n_rep * t.spd, chunk = 8192;
+  std::vector<unsigned char> buf;
+  for (size_t k0 = 0; ok && k0 < n; k0 += chunk) {
+    const size_t m = std::min(chunk, n - k0);
+    buf.resize(m * kLigRecordBytes);
+    for (size_t k = 0; k < m; ++k)
+      std::memcpy(buf.data() + k * kLigRecordBytes, &r[k0 + k], kLigRecordBytes);
+    ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  }
+  if (f && std::fclose(f) != 0) ok = false;
+  if (!ok) t.err.store(1);
+  delete j;
+}
+
+// Copies the completed dump in ring half h out and queues its file.
+gd_status traj_dump(Ens &E, int h) {
+  Traj &t = *E.traj;
+  const size_t w = sizeof(gd_record) * t.spd;
+  GD_CUDA(cudaEventRecord(t.done, E.ctx->stream));
+  GD_CUDA(cudaStreamWaitEvent(t.copy, t.done, 0));
+  GD_CUDA(cudaMemcpy2DAsync(t.host[h], w, t.ring + (size_t)h * t.spd, 2 * w, w, t.n_rep,
+                            cudaMemcpyDeviceToHost, t.copy));
+  GD_CUDA(cudaEventRecord(t.copied[h], t.copy));
+  t.pending[h] = true;
+  DumpJob *j = new (std::nothrow) DumpJob{&t, h, t.seq};
+  if (!j) return fail(GD_ENOMEM, "host allocation");
+  const cudaError_t e = cudaLaunchHostFunc(t.copy, write_dump, j);
+  if (e != cudaSuccess) {
+    delete j;
+    return fail(GD_ECUDA, "cudaLaunchHostFunc: %s", cudaGetErrorString(e));
+  }
+  t.seq += 1;
+  return GD_OK;
+}
+
+gd_status ens_run(Ens &E, int n_steps) {
+  if (n_steps < 0 || n_steps % E.spe != 0)
+    return fail(GD_EINVAL, "n_steps %d is not a multiple of steps_per_exchange %d", n_steps,
+                E.spe);
+  if (E.traj && E.traj->err.load())
+    return fail(GD_EIO, "a trajectory file under %s could not be written", E.traj->dir.c_str());
+  if (n_steps == 0) return GD_OK;
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  cudaStream_t s = E.ctx->stream;
+  GD_CUDA(cudaEventRecord(E.ev0, s));
+  if (!E.traj) {
+    GD_TRY(ens_run_steps(E, n_steps));
+  } else {
+    // segments end at dump boundaries, where the completed dump is copied out
+    Traj &t = *E.traj;
+    for (int left = n_steps; left > 0;) {
+      const int in_dump = E.step % t.spd;
+      const int h = (E.step / t.spd) % 2;
+      const int seg = std::min(left, t.spd - in_dump);
+      if (in_dump == 0 && t.pending[h]) {  // the copy of two dumps ago
+        GD_CUDA(cudaStreamWaitEvent(s, t.copied[h], 0));
+        t.pending[h] = false;
+      }
+      GD_TRY(ens_run_steps(E, seg));
+      left -= seg;
+      if (E.step % t.spd == 0) GD_TRY(traj_dump(E, h));
+    }
+  }
   GD_CUDA(cudaEventRecord(E.ev1, s));
   E.timing = true;
-  E.step += n_steps;
+  return GD_OK;
+}
+
+// Layout descriptor of the dump files (JSON).
+bool write_layout(const Traj &t, const KItem &I) {
+  const std::string path = t.dir + "/" + t.stem + ".layout.json";
+  FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  std::fprintf(f,
+               "{\n"
+               "  \"format\": \"LigRecord dumps: the contents of dataset 'dset' written by "
+               "DumpLigRecord (hdf5io.C), one file per dump, native little-endian\",\n"
+               "  \"files\": \"%s_%%04d.bin\",\n"
+               "  \"dataset\": \"dset\",\n"
+               "  \"shape\": [%d],\n"
+               "  \"element\": {\"name\": \"LigRecord\", \"field\": \"step\", "
+               "\"count\": %d, \"bytes\": %zu},\n"
+               "  \"record\": {\"name\": \"LigRecordSingleStep\", \"bytes\": %zu, "
+               "\"fields\": [\n"
+               "    {\"name\": \"replica.idx_rep\", \"offset\": 0, \"type\": \"int32\"},\n"
+               "    {\"name\": \"replica.idx_prt\", \"offset\": 4, \"type\": \"int32\"},\n"
+               "    {\"name\": \"replica.idx_tmp\", \"offset\": 8, \"type\": \"int32\"},\n"
+               "    {\"name\": \"replica.idx_lig\", \"offset\": 12, \"type\": \"int32\"},\n"
+               "    {\"name\": \"energy.e\", \"offset\": 16, \"type\": \"float32\", "
+               "\"shape\": [%d]},\n"
+               "    {\"name\": \"energy.cmcc\", \"offset\": 56, \"type\": \"float32\"},\n"
+               "    {\"name\": \"movematrix\", \"offset\": 60, \"type\": \"float32\", "
+               "\"shape\": [6]},\n"
+               "    {\"name\": \"step\", \"offset\": 84, \"type\": \"int32\"}]},\n"
+               "  \"steps_per_dump\": %d,\n"
+               "  \"n_rep\": %d, \"n_prt\": %d, \"n_tmp\": %d, \"n_lig\": %d\n"
+               "}\n",
+               t.stem.c_str(), t.n_rep, t.spd, kLigRecordBytes * t.spd, kLigRecordBytes,
+               GD_NTERM, t.spd, t.n_rep, I.n_prt, I.n_tmp, I.n_lig_conf);
+  return std::fclose(f) == 0;
+}
+
+gd_status ens_set_trajectory(Ens &E, const char *dir, const char *stem) {
+  if (!dir || !*dir || !stem || !*stem || std::strchr(stem, '/'))
+    return fail(GD_EINVAL, "trajectory: directory and a file stem without '/' are required");
+  if (E.items.size() != 1) return fail(GD_EINVAL, "trajectory: one complex per run");
+  if (E.traj) return fail(GD_EINVAL, "trajectory: already set");
+  const int spd = E.mc[0].steps_per_dump;
+  if (spd <= 0 || spd % E.spe != 0)
+    return fail(GD_EINVAL, "trajectory: steps_per_dump %d must be a positive multiple of "
+                "steps_per_exchange %d", spd, E.spe);
+  KItem &I = E.items[0];
+  std::unique_ptr<Traj> t(new (std::nothrow) Traj);
+  if (!t) return fail(GD_ENOMEM, "host allocation");
+  t->dir = dir;
+  t->stem = stem;
+  t->spd = spd;
+  t->n_rep = I.n_rep;
+  if (!write_layout(*t, I))
+    return fail(GD_EIO, "trajectory: cannot write %s/%s.layout.json", dir, stem);
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  GD_TRY(dalloc(E, &t->ring, (size_t)I.n_rep * 2 * spd));
+  E.traj = std::move(t);  // freed by ens_free from here on
+  Traj &T = *E.traj;
+  for (gd_record *&h : T.host)
+    GD_CUDA(cudaMallocHost(&h, sizeof(gd_record) * (size_t)I.n_rep * spd));
+  GD_CUDA(cudaStreamCreateWithFlags(&T.copy, cudaStreamNonBlocking));
+  GD_CUDA(cudaEventCreateWithFlags(&T.done, cudaEventDisableTiming));
+  for (cudaEvent_t &e : T.copied) GD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  I.record = T.ring;
+  I.rec_steps = 2 * spd;
+  I.rec_ring = 1;
+  GD_CUDA(cudaMemcpyAsync(E.d_items, E.items.data(), sizeof(KItem) * E.items.size(),
+                          cudaMemcpyHostToDevice, E.ctx->stream));
+  GD_CUDA(cudaStreamSynchronize(E.ctx->stream));
   return GD_OK;
 }
 
@@ -476,6 +666,12 @@ gd_status ens_read(Ens &E, int i, gd_mc_log *log) {
   if (i < 0 || i >= (int)E.items.size()) return fail(GD_EINVAL, "item %d out of range", i);
   GD_CUDA(cudaSetDevice(E.ctx->device));
   GD_TRY(ctx_check(E.ctx));
+  if (E.traj) {  // every queued dump is on disk
+    GD_CUDA(cudaStreamSynchronize(E.traj->copy));
+    if (E.traj->err.load())
+      return fail(GD_EIO, "a trajectory file under %s could not be written",
+                  E.traj->dir.c_str());
+  }
   if (E.timing) {
     float ms = 0.f;
     GD_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
@@ -498,7 +694,7 @@ gd_status ens_read(Ens &E, int i, gd_mc_log *log) {
   if (log->idx_tmp)
     GD_CUDA(cudaMemcpyAsync(log->idx_tmp, E.idx_tmp + b, sizeof(int) * n, cudaMemcpyDeviceToHost,
                             s));
-  if (log->record && I.record)
+  if (log->record && I.record && !I.rec_ring)
     GD_CUDA(cudaMemcpyAsync(log->record, I.record, sizeof(gd_record) * n * std::max(1, I.rec_steps),
                             cudaMemcpyDeviceToHost, s));
   GD_CUDA(cudaStreamSynchronize(s));
@@ -591,6 +787,11 @@ extern "C" gd_status gd_remc_run(gd_remc *r, int n_steps) {
 extern "C" gd_status gd_remc_read(gd_remc *r, gd_mc_log *log) {
   if (!r || !log) return fail(GD_EINVAL, "gd_remc_read: NULL argument");
   return ens_read(r->e, 0, log);
+}
+
+extern "C" gd_status gd_remc_set_trajectory(gd_remc *r, const char *dir, const char *stem) {
+  if (!r) return fail(GD_EINVAL, "remc NULL");
+  return ens_set_trajectory(r->e, dir, stem);
 }
 
 extern "C" gd_status gd_remc_set_profiling(gd_remc *r, int on) {

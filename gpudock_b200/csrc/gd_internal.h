@@ -87,12 +87,14 @@ struct KItem {
   int step0;             // first MC step of the launch when KRun.item_step
   int n_run;             // MC steps of the launch when KRun.item_step
   int spe;               // steps per exchange (exchange kernel, per-item mode)
+  int rec_ring;          // record is a ring of rec_steps steps (slot step %
+  int pad2;              // rec_steps), else steps 0 .. rec_steps-1
   float move_scale[6];
   uint64_t seed;
   uint32_t stream_id, flags;
   const float *minus_beta;  // [n_tmp]
   int *acs_exchg;           // [n_tmp] by slot
-  gd_record *record;        // [n_rep][rec_steps] or nullptr
+  gd_record *record;        // [n_rep][rec_steps] or nullptr (see rec_ring)
   // replica state of this item, indexed by its local replica number
   float *m_old;             // [n_rep][6]
   float *e_old;             // [n_rep][GD_NTERM]

@@ -285,8 +285,9 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
         acc = 1;  // forced accept with beta = 0 (montecarlo_d.cu:236-239)
       } else {
         acc = metropolis(e[9], me.e_old[9], me.mbeta, u01(me.u_bits));
-        if (active && I.record && step < I.rec_steps) {
-          gd_record *rc = I.record + (size_t)rep * I.rec_steps + step;
+        if (active && I.record && (I.rec_ring || step < I.rec_steps)) {
+          const int slot = I.rec_ring ? step % I.rec_steps : step;
+          gd_record *rc = I.record + (size_t)rep * I.rec_steps + slot;
           rc->idx_rep = rep;
           rc->idx_prt = prt_conf;
           rc->idx_tmp = me.idx_tmp;

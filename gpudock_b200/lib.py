@@ -77,6 +77,7 @@ def _declare(lib):
         "gd_remc_destroy": ([P], i32),
         "gd_remc_n_rep": ([P], i32),
         "gd_remc_set_profiling": ([P, i32], i32),
+        "gd_remc_set_trajectory": ([P, C.c_char_p, C.c_char_p], i32),
         "gd_remc_kernel_times": ([P, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                   C.POINTER(C.c_double), C.POINTER(C.c_int)], i32),
         "gd_run": ([C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams), C.POINTER(abi.GdMcLog)], i32),
@@ -278,6 +279,13 @@ class Remc:
 
     def set_profiling(self, on: bool = True):
         check(self.dcx.ctx._lib.gd_remc_set_profiling(self.h, int(on)), "gd_remc_set_profiling")
+
+    def set_trajectory(self, directory: str, stem: str):
+        """Writes every completed dump of steps_per_dump MC steps to
+        {directory}/{stem}_NNNN.bin (see read_trajectory); call before init."""
+        check(self.dcx.ctx._lib.gd_remc_set_trajectory(self.h, os.fsencode(directory),
+                                                       os.fsencode(stem)),
+              "gd_remc_set_trajectory")
 
     def kernel_times(self):
         """(MC-interval ms, launches, exchange ms, launches) since the last call."""
@@ -512,3 +520,31 @@ def schedule_pieces(cost, steps, machines: int):
           "gd_schedule_pieces")
     u = used.value
     return pieces[:off[u]].copy(), off[:u + 1].copy()
+
+
+def trajectory_dtype(layout: dict) -> np.dtype:
+    """numpy structured dtype of one LigRecordSingleStep from a layout file."""
+    rec = layout["record"]
+    names, formats, offsets = [], [], []
+    for f in rec["fields"]:
+        base = {"int32": "<i4", "float32": "<f4"}[f["type"]]
+        names.append(f["name"])
+        formats.append((base, tuple(f["shape"])) if "shape" in f else base)
+        offsets.append(f["offset"])
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets,
+                     "itemsize": rec["bytes"]})
+
+
+def read_trajectory(directory: str, stem: str):
+    """The dump files of a trajectory: a list of [n_rep][steps_per_dump]
+    structured arrays (fields of LigRecordSingleStep), one per dump."""
+    import glob
+    import json
+    with open(os.path.join(directory, stem + ".layout.json")) as f:
+        layout = json.load(f)
+    dt = trajectory_dtype(layout)
+    n_rep, spd = layout["shape"][0], layout["steps_per_dump"]
+    out = []
+    for path in sorted(glob.glob(os.path.join(directory, stem + "_[0-9][0-9][0-9][0-9].bin"))):
+        out.append(np.fromfile(path, dtype=dt).reshape(n_rep, spd))
+    return out

@@ -39,7 +39,8 @@ typedef enum gd_status {
   GD_ECANCELLED = 6,  /* request cancelled before it finished               */
   GD_ENOTFOUND = 7,   /* unknown request id                                 */
   GD_EAGAIN = 8,      /* not finished yet (poll again)                      */
-  GD_ENODEV = 9       /* no CUDA device / kernel image not loadable         */
+  GD_ENODEV = 9,      /* no CUDA device / kernel image not loadable         */
+  GD_EIO = 10         /* a trajectory file could not be written             */
 } gd_status;
 
 /* Thread-local text of the last error raised on this thread. */
@@ -381,6 +382,23 @@ gd_status gd_remc_init(gd_remc *remc);
 gd_status gd_remc_run(gd_remc *remc, int n_steps);
 gd_status gd_remc_read(gd_remc *remc, gd_mc_log *log);
 gd_status gd_remc_destroy(gd_remc *remc);
+/* Trajectory files, the IS_OUTPUT dumps of gpusingle.cu:24-32.  After the
+ * call, every completed dump of mc.steps_per_dump MC steps (a multiple of
+ * steps_per_exchange) is written to {dir}/{stem}_NNNN.bin (NNNN = 0000,
+ * 0001, ...): n_rep LigRecord of steps_per_dump LigRecordSingleStep
+ * (dock.h:487-501; gd_record's first 88 bytes), replica-major, the bytes
+ * DumpLigRecord (hdf5io.C:11-32) stores in dataset "dset".
+ * {dir}/{stem}.layout.json describes that layout (field names, offsets and
+ * types, for a numpy structured dtype or an HDF5 compound type).  The
+ * kernel writes the records into a two-dump device ring; each completed dump
+ * is copied to pinned host memory on a side stream while the next one runs,
+ * and written from there, so the MC steps do not wait for the disk.  Steps
+ * of an unfinished dump are not written.  The in-memory record
+ * (gd_mc_log.record) is not filled while a trajectory is set.  Call before
+ * gd_remc_init; writing errors surface as GD_EIO from gd_remc_run /
+ * gd_remc_read. */
+gd_status gd_remc_set_trajectory(gd_remc *remc, const char *dir,
+                                 const char *stem);
 int gd_remc_n_rep(const gd_remc *remc);
 /* CUDA-event timing of the MC kernels and exchange kernels issued by
  * gd_remc_run / gd_batch_run while profiling is on.  One MC sample spans the
