@@ -22,6 +22,7 @@ MC_EXCHANGE = 0x1
 MC_MOVE_AWAY = 0x2
 MC_RECORD = 0x4
 MC_MCC = 0x8
+MC_BAYES = 0x10
 CMCC_INVALID = 10000.0
 # launch schedules (gd_ctx_set_schedule)
 SCHED_AUTO, SCHED_WAVES, SCHED_PERSISTENT = 0, 1, 2

@@ -81,6 +81,66 @@ __device__ __forceinline__ float decision_expf(float x) {
   return __fmul_rn(__fmul_rn(p, s1), s2);
 }
 
+// ---------------------------------------------------------------------------
+// Bayesian total (IS_BAYE, calcenergy_d.cu:311-347): the densities of
+// util_d.cu:220-290 in the reference's float expressions, with its parameter
+// sets (distribution.h), including its pairing of families and parameters
+// (the low-decoy H-bond density is a normal with the "logistic" parameters,
+// the low-decoy PSP density a logistic with the "Laplace" parameters).
+// ---------------------------------------------------------------------------
+constexpr float kBayesPI = 3.1415926535f;  // PI of size.h
+
+__device__ __forceinline__ float bayes_norm_pdf(float x, float loc, float scale) {
+  const float norm_para = 1.0f / (scale * sqrtf(2.0f * kBayesPI));
+  const float prob = expf(0.0f - (x - loc) * (x - loc) / (2.0f * scale * scale));
+  return norm_para * prob;
+}
+__device__ __forceinline__ float bayes_cauchy_pdf(float x, float loc, float scale) {
+  const float norm_para = 1.0f / (kBayesPI * scale);
+  const float prob = 1.0f / (1.0f + ((x - loc) / scale) * ((x - loc) / scale));
+  return norm_para * prob;
+}
+__device__ __forceinline__ float bayes_logistic_pdf(float x, float loc, float scale) {
+  const float norm_para = 1.0f / scale;
+  const float e_power = expf(-(x - loc) / scale);
+  const float prob = e_power / powf(1.0f + e_power, 2.0f);
+  return norm_para * prob;
+}
+__device__ __forceinline__ float bayes_wald_pdf(float x, float loc, float scale) {
+  const float normed_x = (x - loc) / scale;
+  if (normed_x < 0.0f) return 0.00000001f;
+  const float norm_para = 1.0f / (sqrtf(2.0f * kBayesPI * powf(normed_x, 3.0f)) * scale);
+  const float prob = expf(-powf(normed_x - 1.0f, 2.0f) / (2.0f * normed_x));
+  return norm_para * prob;
+}
+
+// e: the nine normalised terms in rem order (vdw ele pmf psp hdb hpc kde lhm dst).
+__device__ __forceinline__ float bayes_total(const float *e) {
+  const float vdw = e[0], ele = e[1], pmf = e[2], psp = e[3], hdb = e[4], hpc = e[5];
+  const float kde = e[6], lhm = e[7], dst = e[8];
+  const float prob_h =
+      log10f(bayes_norm_pdf(vdw, 0.05286683f, 0.29916642f)) +
+      log10f(bayes_cauchy_pdf(ele, -0.3653806f, 0.00681102f)) +
+      log10f(bayes_logistic_pdf(pmf, -0.0221777f, 0.11847532f)) +
+      log10f(bayes_wald_pdf(hpc, -1.0041231f, 0.1151713f)) +
+      log10f(bayes_norm_pdf(hdb, 0.60986808f, 0.30974999f)) +
+      log10f(bayes_logistic_pdf(dst, -0.8246522f, 0.05218529f)) +
+      log10f(bayes_logistic_pdf(psp, -0.2346999f, 0.09871713f)) +
+      log10f(bayes_wald_pdf(kde, -1.0112055f, 0.09882933f)) +
+      log10f(bayes_logistic_pdf(lhm, -0.3377100f, 0.09282947f));
+  const float prob_l =
+      log10f(bayes_norm_pdf(vdw, 0.15818486f, 0.29032471f)) +
+      log10f(bayes_cauchy_pdf(ele, -0.3647824f, 0.00534225f)) +
+      log10f(bayes_logistic_pdf(pmf, 0.04257942f, 0.08801551f)) +
+      log10f(bayes_wald_pdf(hpc, -1.0019512f, 0.10312611f)) +
+      log10f(bayes_norm_pdf(hdb, 0.76967708f, 0.11224029f)) +
+      log10f(bayes_logistic_pdf(dst, -0.7509618f, 0.08757299f)) +
+      log10f(bayes_logistic_pdf(psp, -0.2022064f, 0.07854212f)) +
+      log10f(bayes_wald_pdf(kde, -1.004605f, 0.02967548f)) +
+      log10f(bayes_logistic_pdf(lhm, -0.2387023f, 0.12134983f));
+  return prob_l - prob_h;
+}
+
 // Metropolis rule (accept_d.cu:19-23) on given totals.
 __device__ __forceinline__ int metropolis(float e_new, float e_old, float minus_beta, float u) {
   const float de = __fsub_rn(e_new, e_old);

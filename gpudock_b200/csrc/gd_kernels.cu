@@ -253,6 +253,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
     float tot = __fmul_rn(T.w[0], e[0]);
 #pragma unroll
     for (int i = 1; i < 9; ++i) tot = __fadd_rn(tot, __fmul_rn(T.w[i], e[i]));
+    if (MODE != KMODE_POSES && (I.flags & GD_MC_BAYES)) tot = bayes_total(e);
     e[9] = tot;
     if (MODE != KMODE_POSES && (I.flags & GD_MC_MCC)) {
       // confusion counts against the reference map (calcmcc_d.cu:189-206);

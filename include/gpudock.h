@@ -326,6 +326,13 @@ gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *dcx,
  * gd_record.cmcc; it never enters the acceptance. */
 #define GD_MC_MCC        0x8u
 #define GD_CMCC_INVALID  10000.0f
+/* Bayesian total (IS_BAYE, calcenergy_d.cu:311-347): e[GD_E_TOTAL] =
+ * sum of log10 densities of the nine normalised terms under the low-decoy
+ * distributions minus the same under the high-decoy distributions
+ * (families and parameters of util_d.cu:220-290 and distribution.h), in
+ * place of the weighted sum.  It is the energy the Metropolis test and the
+ * exchange use. */
+#define GD_MC_BAYES      0x10u
 
 typedef struct gd_mc_params {
   int steps_total;           /* MC steps per replica                        */

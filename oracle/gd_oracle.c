@@ -375,6 +375,72 @@ void orc_energy_coords(const gd_complex *cx, int prt_conf, const float *lx,
   for (int i = 0; i < GD_NTERM; ++i) terms[i] = e[i];
 }
 
+/* Bayesian total of IS_BAYE (calcenergy_d.cu:311-347): densities of
+ * util_d.cu:220-290 (NormPdf, CauchyPdf, LogisticPdf, WaldPdf) with the
+ * parameters of distribution.h, in the reference's float expressions and
+ * pairings (low H-bond: normal density, "logistic" parameters; low PSP:
+ * logistic density, "Laplace" parameters); libm's expf/powf/sqrtf/log10f. */
+static const float kBayesPI = 3.1415926535f; /* PI of size.h */
+
+static float bayes_norm(float x, float loc, float scale)
+{
+  const float norm_para = 1.0f / (scale * sqrtf(2.0f * kBayesPI));
+  const float prob = expf(0.0f - (x - loc) * (x - loc) / (2.0f * scale * scale));
+  return norm_para * prob;
+}
+
+static float bayes_cauchy(float x, float loc, float scale)
+{
+  const float norm_para = 1.0f / (kBayesPI * scale);
+  const float prob = 1.0f / (1.0f + ((x - loc) / scale) * ((x - loc) / scale));
+  return norm_para * prob;
+}
+
+static float bayes_logistic(float x, float loc, float scale)
+{
+  const float norm_para = 1.0f / scale;
+  const float e_power = expf(-(x - loc) / scale);
+  const float prob = e_power / powf(1.0f + e_power, 2.0f);
+  return norm_para * prob;
+}
+
+static float bayes_wald(float x, float loc, float scale)
+{
+  const float normed_x = (x - loc) / scale;
+  if (normed_x < 0.0f) return 0.00000001f;
+  const float norm_para = 1.0f / (sqrtf(2.0f * kBayesPI * powf(normed_x, 3.0f)) * scale);
+  const float prob = expf(-powf(normed_x - 1.0f, 2.0f) / (2.0f * normed_x));
+  return norm_para * prob;
+}
+
+/* e: the nine normalised terms (vdw ele pmf psp hdb hpc kde lhm dst) */
+float orc_bayes_total(const float *e)
+{
+  const float vdw = e[0], ele = e[1], pmf = e[2], psp = e[3], hdb = e[4];
+  const float hpc = e[5], kde = e[6], lhm = e[7], dst = e[8];
+  const float prob_h =
+      log10f(bayes_norm(vdw, 0.05286683f, 0.29916642f)) +
+      log10f(bayes_cauchy(ele, -0.3653806f, 0.00681102f)) +
+      log10f(bayes_logistic(pmf, -0.0221777f, 0.11847532f)) +
+      log10f(bayes_wald(hpc, -1.0041231f, 0.1151713f)) +
+      log10f(bayes_norm(hdb, 0.60986808f, 0.30974999f)) +
+      log10f(bayes_logistic(dst, -0.8246522f, 0.05218529f)) +
+      log10f(bayes_logistic(psp, -0.2346999f, 0.09871713f)) +
+      log10f(bayes_wald(kde, -1.0112055f, 0.09882933f)) +
+      log10f(bayes_logistic(lhm, -0.3377100f, 0.09282947f));
+  const float prob_l =
+      log10f(bayes_norm(vdw, 0.15818486f, 0.29032471f)) +
+      log10f(bayes_cauchy(ele, -0.3647824f, 0.00534225f)) +
+      log10f(bayes_logistic(pmf, 0.04257942f, 0.08801551f)) +
+      log10f(bayes_wald(hpc, -1.0019512f, 0.10312611f)) +
+      log10f(bayes_norm(hdb, 0.76967708f, 0.11224029f)) +
+      log10f(bayes_logistic(dst, -0.7509618f, 0.08757299f)) +
+      log10f(bayes_logistic(psp, -0.2022064f, 0.07854212f)) +
+      log10f(bayes_wald(kde, -1.004605f, 0.02967548f)) +
+      log10f(bayes_logistic(lhm, -0.2387023f, 0.12134983f));
+  return prob_l - prob_h;
+}
+
 /* Energy of one pose (move vector) of ligand conformation lig_conf. */
 void orc_energy_pose(const gd_complex *cx, int prt_conf, int lig_conf,
                      const float m[6], double raw[GD_NRAW],
@@ -524,6 +590,7 @@ static int orc_mc_step(const gd_complex *cx, const gd_mc_params *mc, int n_lig,
   float e_new[GD_NTERM];
   orc_energy_coords(cx, p, buf, buf + lna, buf + 2 * lna, center, raw, e_new,
                     NULL);
+  if (mc->flags & GD_MC_BAYES) e_new[GD_E_TOTAL] = orc_bayes_total(e_new);
   const float mb = mc->minus_beta[st->idx_tmp];
   const float de = e_new[GD_E_TOTAL] - st->e_old[GD_E_TOTAL];
   const int acc = orc_u01(o1[2]) < orc_expf(de * mb);
@@ -647,6 +714,7 @@ int orc_remc_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log,
       double raw[GD_NRAW];
       orc_energy_coords(cx, p, buf, buf + lna, buf + 2 * lna, center, raw,
                         st->e_old, NULL);
+      if (mc->flags & GD_MC_BAYES) st->e_old[GD_E_TOTAL] = orc_bayes_total(st->e_old);
       st->cmcc = mcc_ref ? orc_mcc_of(cx, p, buf, buf + lna, buf + 2 * lna, mcc_ref) : 0.0f;
       /* forced accept with beta = 0 (montecarlo_d.cu:236-239) */
       memcpy(st->m_old, m, sizeof(m));

@@ -59,6 +59,8 @@ def load(native: bool = False):
     lib.orc_max_threads.restype = C.c_int
     lib.orc_mcc.argtypes = [C.POINTER(abi.GdComplex), C.c_int, C.c_int, C.c_int, P]
     lib.orc_mcc.restype = C.c_float
+    lib.orc_bayes_total.argtypes = [P]
+    lib.orc_bayes_total.restype = C.c_float
     _libs[key] = lib
     return lib
 
@@ -155,3 +157,14 @@ def mcc(cx: abi.Complex, ref_prt: int, prt_conf: int, lig_conf: int, m) -> float
     mv = np.ascontiguousarray(m, np.float32).reshape(6)
     return float(load().orc_mcc(C.byref(cx.struct()), ref_prt, prt_conf, lig_conf,
                                 mv.ctypes.data))
+
+
+def bayes_total(e) -> np.ndarray:
+    """Bayesian total (IS_BAYE) of normalised terms e[..., :9] (rem order)."""
+    e = np.ascontiguousarray(e, np.float32).reshape(-1, np.shape(e)[-1])
+    lib = load()
+    out = np.empty(len(e), np.float32)
+    for i in range(len(e)):
+        row = np.ascontiguousarray(e[i, :9])
+        out[i] = lib.orc_bayes_total(row.ctypes.data)
+    return out

@@ -115,6 +115,58 @@ def test_oracle_remc_runs_and_counts():
     assert (rec["step"] == np.arange(40)).all()
 
 
+def _bayes_reference_f64(e):
+    """IS_BAYE total from scipy's standard densities (float64): normal,
+    Cauchy, logistic and Wald (inverse Gaussian with mean 1) in loc/scale
+    form, with the parameter sets and pairings of distribution.h and
+    calcenergy_d.cu:311-347 (low H-bond: normal with the "logistic"
+    parameters; low PSP: logistic with the "Laplace" parameters; a Wald
+    argument below loc has density 1e-8).  The parameters are the
+    reference's float literals, so they are rounded to float32 first: near
+    a Wald location the rounding of loc alone moves log10 by ~1e-4."""
+    from scipy import stats as st
+
+    def f32(v):
+        return float(np.float32(v))
+
+    def norm(x, loc, scale):
+        return st.norm.pdf(x, f32(loc), f32(scale))
+
+    def cauchy(x, loc, scale):
+        return st.cauchy.pdf(x, f32(loc), f32(scale))
+
+    def logistic(x, loc, scale):
+        return st.logistic.pdf(x, f32(loc), f32(scale))
+
+    def wald(x, loc, scale):
+        return st.wald.pdf(x, f32(loc), f32(scale)) if x >= f32(loc) else 1e-8
+
+    vdw, ele, pmf, psp, hdb, hpc, kde, lhm, dst = (float(v) for v in e[:9])
+    high = [norm(vdw, 0.05286683, 0.29916642), cauchy(ele, -0.3653806, 0.00681102),
+            logistic(pmf, -0.0221777, 0.11847532), wald(hpc, -1.0041231, 0.1151713),
+            norm(hdb, 0.60986808, 0.30974999), logistic(dst, -0.8246522, 0.05218529),
+            logistic(psp, -0.2346999, 0.09871713), wald(kde, -1.0112055, 0.09882933),
+            logistic(lhm, -0.3377100, 0.09282947)]
+    low = [norm(vdw, 0.15818486, 0.29032471), cauchy(ele, -0.3647824, 0.00534225),
+           logistic(pmf, 0.04257942, 0.08801551), wald(hpc, -1.0019512, 0.10312611),
+           norm(hdb, 0.76967708, 0.11224029), logistic(dst, -0.7509618, 0.08757299),
+           logistic(psp, -0.2022064, 0.07854212), wald(kde, -1.004605, 0.02967548),
+           logistic(lhm, -0.2387023, 0.12134983)]
+    lh, ll = np.log10(high), np.log10(low)
+    return ll.sum() - lh.sum(), np.abs(lh).sum() + np.abs(ll).sum()
+
+
+def test_oracle_bayes_total_matches_standard_densities():
+    rng = np.random.default_rng(12)
+    locs = np.array([0.1, -0.365, 0.0, -0.22, 0.7, -0.95, -0.9, -0.3, -0.8], np.float32)
+    e = (locs + rng.normal(0, 0.1, (200, 9))).astype(np.float32)
+    e[:5, 5] = -1.2  # Wald below its loc: density 1e-8
+    got = orc.bayes_total(e)
+    for row, g in zip(e, got):
+        ref, mag = _bayes_reference_f64(row)
+        assert abs(float(g) - ref) <= 2e-6 * mag + 1e-5, (row, g, ref)
+
+
 def test_oracle_mcc_bookkeeping():
     """GD_MC_MCC in the oracle's REMC driver: every recorded value is the MCC of
     the recorded (accepted) pose; the start pose of ligand conformation 0 against
