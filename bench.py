@@ -165,6 +165,17 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
                       f"{'-march=native' if native else 'x86-64'} OpenMP build)"}
 
 
+def profile_metric(workload, key):
+    """(value, unit) of one metric row of the committed ncu summary of the
+    headline kernel of this workload, or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", f"dock_kernel_remc_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"`" + re.escape(key) + r"`\) \| ([0-9.]+) ?([%\w]*)", open(path).read())
+    return (float(m.group(1)), m.group(2)) if m else None
+
+
 def profile_traffic(workload):
     """DRAM bytes per launch of the headline kernel from the committed ncu
     summary of this workload (dram__bytes_read.sum + dram__bytes_write.sum),
@@ -544,6 +555,16 @@ def main():
                          "traffic": profile_traffic(w.name),
                          "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per "
                                            "launch, ncu capture summarised in profiles/",
+                         "ncu_pipe_util_pct": {
+                             "fma": profile_metric(
+                                 w.name,
+                                 "sm__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active"),
+                             "xu": profile_metric(
+                                 w.name,
+                                 "sm__inst_executed_pipe_xu.avg.pct_of_peak_sustained_active"),
+                             "note": "FP32 (FMA) and MUFU (XU) pipe utilisation of the same "
+                                     "kernel from the committed ncu capture; frac counts the 36 "
+                                     "algorithmic flops per pair against the FFMA peak"},
                          "kernel": "dock_kernel<REMC> (MC interval)",
                          "flops_per_launch": FLOP_PER_PAIR * pairs_per_launch,
                          "mean_launch_ms": mean_launch_s * 1e3, "launches": mc_n,
