@@ -44,6 +44,12 @@ def _declare(lib):
         "gd_autotune": ([P, P, C.POINTER(abi.GdTile), C.POINTER(C.c_double)], i32),
         "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
         "gd_ctx_set_schedule": ([P, i32, i32], i32),
+        "gd_load": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                     C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara), C.c_uint,
+                     C.POINTER(P)], i32),
+        "gd_loaded_complex": ([P, C.POINTER(abi.GdComplex)], i32),
+        "gd_loaded_ligand_id": ([P], C.c_char_p),
+        "gd_loaded_free": ([P], i32),
         "gd_schedule_pieces": ([C.POINTER(C.c_double), C.POINTER(C.c_int), i32, i32,
                                 C.POINTER(C.c_int), i32, C.POINTER(C.c_int),
                                 C.POINTER(C.c_int)], i32),
@@ -548,3 +554,56 @@ def read_trajectory(directory: str, stem: str):
     for path in sorted(glob.glob(os.path.join(directory, stem + "_[0-9][0-9][0-9][0-9].bin"))):
         out.append(np.fromfile(path, dtype=dt).reshape(n_rep, spd))
     return out
+
+
+LOAD_PEPTIDE_ALL_MODELS = 0x1
+
+
+def load_files(pdb: str, sdf: str, lhm: str, ligand_id: str, molid: str = "MOLID",
+               raw: "abi.GdEneparaRaw | None" = None, flags: int = 0) -> abi.Complex:
+    """A complex from the reference's input files (gd_load: loadProtein,
+    loadLigand, loadLHM and the table derivation linear_dock runs), copied
+    into numpy arrays.  raw: force field (default: the packaged one);
+    flags: LOAD_PEPTIDE_ALL_MODELS (see gd_load)."""
+    from . import forcefield
+    lib = load()
+    if raw is None:
+        raw = forcefield.raw_struct(forcefield.load_raw())
+    ff = enepara_optimize(raw)
+    h = C.c_void_p()
+    check(lib.gd_load(os.fsencode(pdb), os.fsencode(sdf), os.fsencode(lhm),
+                      ligand_id.encode(), molid.encode(), C.byref(raw), C.byref(ff),
+                      int(flags), C.byref(h)), "gd_load")
+    try:
+        v = abi.GdComplex()
+        check(lib.gd_loaded_complex(h, C.byref(v)), "gd_loaded_complex")
+
+        def arr(ptr, n, dt):
+            if not n:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
+
+        def xyz(x, y, z, n, shape):
+            return np.stack([arr(x, n, np.float32), arr(y, n, np.float32),
+                             arr(z, n, np.float32)], axis=-1).reshape(*shape, 3)
+
+        lg, pr, pk, mc = v.lig, v.prt, v.kde, v.mcs
+        lna, nl, pnp, npr, nf = lg.lna, lg.n_conf, pr.pnp, pr.n_conf, mc.n_field
+        cx = abi.Complex(
+            lig_xyz=xyz(lg.x, lg.y, lg.z, nl * lna, (nl, lna)),
+            lig_t=arr(lg.t, lna, np.int32), lig_c=arr(lg.c, lna, np.float32),
+            lig_n=arr(lg.n, lna, np.int32), lig_center=np.array(lg.center[:], np.float32),
+            prt_xyz=xyz(pr.x, pr.y, pr.z, npr * pnp, (npr, pnp)),
+            prt_t=arr(pr.t, pnp, np.int32), prt_c=arr(pr.c, pnp, np.int32),
+            prt_ele=arr(pr.ele, pnp, np.float32), prt_seq3r=arr(pr.seq3r, pnp, np.int32),
+            prt_hpcflag=arr(pr.c0_and_d12_or_c2, pnp, np.int32),
+            prt_hpp=arr(pr.hpp, pnp, np.float32),
+            pocket_center=np.array(pr.pocket_center[:], np.float32),
+            psp=arr(v.psp.psp, abi.NLT * v.psp.n_col, np.float32).reshape(abi.NLT, v.psp.n_col),
+            kde_xyz=xyz(pk.x, pk.y, pk.z, pk.pnk, (pk.pnk,)), kde_t=arr(pk.t, pk.pnk, np.int32),
+            mcs_xyz=xyz(mc.x, mc.y, mc.z, mc.pos * nf, (mc.pos, nf)),
+            mcs_tcc=arr(mc.tcc, mc.pos, np.float32), ff=ff)
+        cx.ligand_id = (lib.gd_loaded_ligand_id(h) or b"").decode()
+        return cx
+    finally:
+        lib.gd_loaded_free(h)

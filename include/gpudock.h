@@ -15,6 +15,8 @@
  *   OptimizeEnepara  gpudocksm-rem-1.2/src/util.C:405-458
  *   SetTemperature   gpudocksm-rem-1.2/src/util.C:491-532
  *   SetReplica       gpudocksm-rem-1.2/src/util.C:538-558
+ *   loadProtein / loadLigand / loadLHM
+ *                    gpudocksm-rem-1.2/src/load.C:100-420, 595-990, 1011-1126
  */
 #ifndef GPUDOCK_H
 #define GPUDOCK_H
@@ -40,7 +42,7 @@ typedef enum gd_status {
   GD_ENOTFOUND = 7,   /* unknown request id                                 */
   GD_EAGAIN = 8,      /* not finished yet (poll again)                      */
   GD_ENODEV = 9,      /* no CUDA device / kernel image not loadable         */
-  GD_EIO = 10         /* a trajectory file could not be written             */
+  GD_EIO = 10         /* a file could not be read or written                */
 } gd_status;
 
 /* Thread-local text of the last error raised on this thread. */
@@ -196,6 +198,43 @@ typedef struct gd_complex {
 
 /* Checks every size, type code and index of a complex. */
 gd_status gd_complex_validate(const gd_complex *cx);
+
+/* ------------------------------------------------------------------------ */
+/* Input files (host): the loaders of load.C and the table derivation of     */
+/* util.C:200-458 that linear_dock runs before Run.                          */
+/* ------------------------------------------------------------------------ */
+/* A loaded complex owns its arrays; gd_loaded_complex gives the gd_complex
+ * view of them (valid until gd_loaded_free).
+ *  pdb:  protein ensemble, MODEL/ENDMDL models; each residue becomes its CA
+ *        point, a peptide-plane point and its side-chain points, each the
+ *        mean of its atoms per model (loadProtein, load.C:595-990).
+ *  sdf:  ligand, one SD record: the atom block gives the default pose, the
+ *        OB_ATOM_TYPES / OB_ATOMIC_CHARGES properties types and charges, and
+ *        ENSEMBLE_COORDS one conformation per line; conformations within
+ *        0.1 A RMSD of the default pose (after optimal superposition) are
+ *        dropped, at most 70 are kept (loadLigand, load.C:100-420);
+ *        molid is the property tag of the ligand id ("MOLID").
+ *  lhm:  pocket template .ff: KDE points, PSP entries and the MCS records
+ *        whose ligand id is ligand_id (loadLHM, load.C:1011-1126).
+ *  raw:  force field (its ele and hpp tables give the points' ele and hpp,
+ *        CopyProteinResidue util.C:253-275).
+ *  ff:   the kernel-ready force field the gd_complex view points to.
+ * Unreadable files give GD_EIO, malformed content GD_EINVAL. */
+typedef struct gd_loaded gd_loaded;
+/* The peptide-plane point of a residue (previous residue's C and O, this
+ * residue's N) in every model.  Without the flag the points of models after
+ * the second are as the reference's loader makes them: from the N atom
+ * alone (it looks the previous residue up in a conformation it has not
+ * filled yet, load.C:822-833, and finds serial 0 in zeroed memory). */
+#define GD_LOAD_PEPTIDE_ALL_MODELS 0x1u
+gd_status gd_load(const char *pdb, const char *sdf, const char *lhm,
+                  const char *ligand_id, const char *molid,
+                  const gd_enepara_raw *raw, const gd_enepara *ff,
+                  unsigned flags, gd_loaded **out);
+gd_status gd_loaded_complex(const gd_loaded *loaded, gd_complex *out);
+/* The ligand id read from the SD record (empty if none). */
+const char *gd_loaded_ligand_id(const gd_loaded *loaded);
+gd_status gd_loaded_free(gd_loaded *loaded);
 
 /* ------------------------------------------------------------------------ */
 /* Device context and device-resident complexes                             */
