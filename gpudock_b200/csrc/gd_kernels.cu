@@ -465,39 +465,49 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
                                             bool mcc_on, int p, double *my_red) {
   const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
   const bool hflag = (meta & META_HPC_BIT) != 0u;
+  // the largest squared distance at which a term below can fire for this
+  // point: atom pairs that no lane has within it are skipped (warp-uniform);
+  // in practice a few percent of a close point's atom pairs are in range
+  const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f,
+                                             (is_c2 || mcc_on) ? T.near_mcc2 : 0.0f));
 #pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    const float2 ax = nx[k >> 1], ay = ny[k >> 1], az = nz[k >> 1];
-    const float dx = (k & 1) ? ax.y + Ap.x : ax.x + Ap.x;
-    const float dy = (k & 1) ? ay.y + Ap.y : ay.x + Ap.y;
-    const float dz = (k & 1) ? az.y + Ap.z : az.x + Ap.z;
-    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (hflag && d2 <= 81.0f && k < n_my) {
-      float *hh = my_hpc + (size_t)A * k * 32;
-      *hh = fmaf(hpp, hpc_poly(d2), *hh);
-    }
-    // the distance itself only where a switch can be near (d^2 bounds with
-    // margin: the tests below decide on d exactly as before)
-    if (d2 <= T.near_ele2) {
-      const float rk = frsqrt(d2);
-      const float s1 = T.el1 * (d2 * rk);
-      if (s1 < 1.0f) {
-        const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
-        fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
+  for (int h = 0; h < NA / 2; ++h) {
+    const float2 dx2 = add2(nx[h], dup2(Ap.x));
+    const float2 dy2 = add2(ny[h], dup2(Ap.y));
+    const float2 dz2 = add2(nz[h], dup2(Ap.z));
+    const float2 d2p = fma2(dx2, dx2, fma2(dy2, dy2, mul2(dz2, dz2)));
+    if (!__any_sync(0xffffffffu, fminf(d2p.x, d2p.y) <= thr)) continue;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int k = 2 * h + j;
+      const float d2 = j ? d2p.y : d2p.x;
+      if (hflag && d2 <= 81.0f && k < n_my) {
+        float *hh = my_hpc + (size_t)A * k * 32;
+        *hh = fmaf(hpp, hpc_poly(d2), *hh);
       }
-    }
-    if ((is_c2 || mcc_on) && k < n_my && d2 <= T.near_mcc2) {
-      const float d = d2 * frsqrt(d2);
-      const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
-      const float dm = d + ((k & 1) ? T1.y : T1.x);
-      if (dm <= 0.0f) {
-        if (is_c2)
-          fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + (meta >> META_SEQ_SHIFT)]);
-        if (mcc_on) {
-          const int a = s_atom[ag + A * k];
-          my_red[8 * 32] += 1.0;
-          if ((__ldg(&T.mcc_ref[(size_t)a * T.mcc_words + (p >> 5)]) >> (p & 31)) & 1u)
-            my_red[9 * 32] += 1.0;
+      // the distance itself only where a switch can be near (d^2 bounds with
+      // margin: the tests below decide on d exactly as before)
+      if (d2 <= T.near_ele2) {
+        const float rk = frsqrt(d2);
+        const float s1 = T.el1 * (d2 * rk);
+        if (s1 < 1.0f) {
+          const float gnear = fmaf(s1 * s1, fmaf(T.b1, s1, T.a1), T.el0);
+          fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
+        }
+      }
+      if ((is_c2 || mcc_on) && k < n_my && d2 <= T.near_mcc2) {
+        const float d = d2 * frsqrt(d2);
+        const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
+        const float dm = d + ((k & 1) ? T1.y : T1.x);
+        if (dm <= 0.0f) {
+          if (is_c2)
+            fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + (meta >> META_SEQ_SHIFT)]);
+          if (mcc_on) {
+            const int a = s_atom[ag + A * k];
+            my_red[8 * 32] += 1.0;
+            if ((__ldg(&T.mcc_ref[(size_t)a * T.mcc_words + (p >> 5)]) >> (p & 31)) & 1u)
+              my_red[9 * 32] += 1.0;
+          }
         }
       }
     }
