@@ -385,16 +385,16 @@ __device__ __forceinline__ void pair_hh(const bool hdb, float2 nx, float2 ny, fl
   const float2 r2 = mul2(r, r);
   const float2 r3 = mul2(r2, r);
   const float2 r6 = mul2(r3, r3);
-  const float2 r9 = mul2(r6, r3);
-  const float2 p1 = mul2(lo2(T0), r9);
+  const float2 t9 = mul2(lo2(T0), r3);  // p1a r^3, beside r^6
+  const float2 p1 = mul2(t9, r6);
   const float2 p12 = fma2(hi2(T0), r6, p1);  // p1 - p2
   const float2 p4 = fma2(p1, fma2(K.lj1, d2, K.lj0), K.one);
   const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
   const float2 ex = make_float2(fex2(arg.x), fex2(arg.y));
-  const float2 e1 = add2(ex, K.one);
-  const float2 den = mul2(p4, e1);
+  // D1 D2 and num1 D2 as single FMAs: p4 (1 + ex) = p4 ex + p4
+  const float2 den = fma2(p4, ex, p4);
   const float2 inv = make_float2(frcp(den.x), frcp(den.y));
-  fvdw = fma2(mul2(p12, e1), inv, fvdw);
+  fvdw = fma2(fma2(p12, ex, p12), inv, fvdw);
   fpmf = fma2(mul2(hi2(T1), p4), inv, fpmf);
   fek = fma2(dup2(Ap.w), r, fek);
   mn = fminf(mn, fminf(d2.x, d2.y));
