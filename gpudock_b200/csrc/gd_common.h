@@ -105,8 +105,10 @@ Tile tile_for(gd_ctx *ctx, const KTables &T);
 // streams (n <= kMaxSide; the first is ctx->stream) that start after the work
 // already queued on ctx->stream; join_streams makes ctx->stream wait for all
 // of them.  Both work inside a stream capture, which turns the plans into
-// parallel graph branches.
-constexpr int kMaxSide = 8;
+// parallel graph branches.  Plans beyond kMaxSide share streams (and run
+// after the plan they share one with), so it covers every launch-shape class
+// a batch can have in practice.
+constexpr int kMaxSide = 32;
 gd_status fork_streams(gd_ctx *c, int n, cudaStream_t *out);
 gd_status join_streams(gd_ctx *c, int n);
 }  // namespace gd

@@ -344,6 +344,9 @@ gd_status ens_prepare(Ens &E, int n_steps) {
   const int mode = E.ctx->sched_mode;
   if (mode == GD_SCHED_WAVES || n_steps < 2) return GD_OK;
   for (Plan &pl : E.plans) {
+    // each plan as if it had the GPU to itself: plans that run side by side
+    // are balanced better by the hardware's dynamic CTA placement than by
+    // static shares of the SMs (measured on the batched form)
     if (pl.auto_machines == 0) {
       KRun R = run_desc(E, pl, KMODE_REMC);
       int occ = 0;
