@@ -525,7 +525,10 @@ def main():
         for name, fn in (("plain", lambda: form_plain(ctx, stream, args.seed, flush)),
                          ("batched", lambda: form_batched(ctx, stream, args.seed, flush)),
                          ("poses", lambda: form_poses(ctx, stream, args.seed)),
-                         ("served", lambda: form_served(args.seed))):
+                         ("served", lambda: form_served(args.seed)),
+                         # the top of the trace's rate range: the requests arrive
+                         # faster than they finish, so this measures capacity
+                         ("served_400", lambda: form_served(args.seed, rate=400.0))):
             try:
                 forms[name] = fn()
             except Exception as exc:  # reported, not fatal
