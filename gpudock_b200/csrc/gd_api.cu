@@ -68,11 +68,12 @@ Tile default_tile(int lna) {
   return best;
 }
 
-void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident) {
+void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident, int split) {
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  const int own = (n_tiles + split - 1) / split;  // tiles of a split's busiest CTA
   const size_t limit = 227 * 1024;
-  if (n_tiles <= MAX_RESIDENT_TILES && dock_smem_bytes(t.A, t.P, t.NA, n_tiles) <= limit) {
-    *n_stages = n_tiles;
+  if (own <= MAX_RESIDENT_TILES && dock_smem_bytes(t.A, t.P, t.NA, own, split) <= limit) {
+    *n_stages = own;
     *resident = 1;
   } else {
     *n_stages = STREAM_STAGES;
@@ -81,6 +82,15 @@ void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident) 
 }
 
 int lna_bucket(int lna) { return std::min(((lna + 7) / 8) * 8, MAX_LNA); }
+
+int split_for(gd_ctx *ctx, const KTables &T) {
+  if (ctx->split_mode > 0) return ctx->split_mode;
+  // the largest power of two <= cost / kSplitCost, at most 8
+  const double cost = (double)lna_bucket(T.lna) * T.pnp;
+  int k = 1;
+  while (k < 8 && cost >= kSplitCost * 2.0 * k) k *= 2;
+  return k;
+}
 
 Tile tile_for(gd_ctx *ctx, const KTables &T) {
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
@@ -776,6 +786,14 @@ extern "C" gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines) {
   if (machines < 0) return fail(GD_EINVAL, "gd_ctx_set_schedule: machines=%d", machines);
   ctx->sched_mode = mode;
   ctx->sched_machines = machines;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_ctx_set_split(gd_ctx *ctx, int split) {
+  if (!ctx) return fail(GD_EINVAL, "gd_ctx_set_split: NULL context");
+  if (split < 0 || split > 8 || (split & (split - 1)))
+    return fail(GD_EINVAL, "gd_ctx_set_split: %d is not 0, 1, 2, 4 or 8", split);
+  ctx->split_mode = split;
   return GD_OK;
 }
 

@@ -48,7 +48,9 @@ constexpr int kNAValues[] = {2, 4, 6, 8, 10};
 
 Tile default_tile(int lna);
 int round_na(int na);  // smallest compiled NA >= na (0 if none)
-void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident);
+// Resident staging when the tiles of one CTA (of a split's busiest CTA) fit
+// in shared memory, else the streaming ring.
+void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident, int split = 1);
 
 }  // namespace gd
 
@@ -64,6 +66,7 @@ struct gd_ctx {
   int n_sm = 148;
   int sched_mode = 0;      // GD_SCHED_*
   int sched_machines = 0;  // persistent CTAs (0: SMs x occupancy)
+  int split_mode = 0;      // CTAs per unit of MC launches (0: split_for's rule)
   std::atomic<int> refs{1};
   // autotuned launch shapes keyed by (ligand-size bucket, protein tiles)
   std::mutex tile_mu;
@@ -98,6 +101,11 @@ gd_status kernel_error(int code);
 // shapes are chosen (and autotuned) per bucket and cover its largest size.
 int lna_bucket(int lna);
 Tile tile_for(gd_ctx *ctx, const KTables &T);
+// CTAs (a thread-block cluster) that share each 32-replica unit of a complex
+// in MC launches: a function of the complex alone (ligand-size bucket x
+// protein points), so its runs are the same in any mix; 1 below 2 kSplitCost.
+constexpr double kSplitCost = 150000.0;
+int split_for(gd_ctx *ctx, const KTables &T);
 
 // Launches of different shapes (one per launch plan) are independent; each
 // kernel holds one CTA per SM, so a plan with fewer CTAs than SMs leaves the

@@ -225,6 +225,27 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Thread-block cluster: this CTA's rank, a barrier over every thread of the
+// cluster (release / acquire: shared-memory writes before it are visible to
+// the cluster's other CTAs after it), and the generic address of the same
+// shared-memory location in the cluster's CTA `rank` (distributed shared
+// memory).
+__device__ __forceinline__ int cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return (int)r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;"
+               ::: "memory");
+}
+template <typename T>
+__device__ __forceinline__ const T *cluster_map(const T *p, int rank) {
+  uint64_t out;
+  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"((uint64_t)p), "r"(rank));
+  return reinterpret_cast<const T *>(out);
+}
+
 // Release store / acquire load of a word at GPU scope (progress flags
 // between CTAs of one launch).
 __device__ __forceinline__ void st_release(int *p, int v) {

@@ -41,6 +41,7 @@ struct Plan {
   double cost = 0.0;  // sum over its CTAs of ligand atoms x protein points
   int n_stages = 0, resident = 0, group_major = 0, fused = 0, grid = 0;
   int hb_pairs = 0;  // largest hb_pairs_of over its items
+  int split = 1;     // CTAs (a cluster) per unit (split_for)
   int *d_cta_item = nullptr, *d_cta_rep0 = nullptr, *d_cta_nrep = nullptr;
   // persistent schedules (KRun.pieces) of this plan's units, by launch length
   std::vector<double> unit_cost;  // [grid] cost of one MC step of each unit
@@ -242,21 +243,23 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
   GD_TRY(dcopy(E, &E.d_items, E.items));
 
   // launch plans: one per (shape, staging, layout); CTAs in decreasing cost
-  using Key = std::tuple<int, int, int, int, int, int>;
+  using Key = std::tuple<int, int, int, int, int, int, int>;
   std::map<Key, std::vector<std::tuple<double, int, int, int>>> ctas;  // cost, item, rep0, n
   std::map<Key, Plan> plans;
   std::vector<KGroup> groups;
   for (int i = 0; i < n; ++i) {
     const KItem &I = E.items[i];
     Tile t = tile_for(ctx, I.T);
+    const int split = split_for(ctx, I.T);
     int ns, res;
-    pick_stages(I.T, t, &ns, &res);
+    pick_stages(I.T, t, &ns, &res, split);
     const int nt = I.n_tmp, nl = I.n_lig_conf;
     const bool gm = (32 % nt) == 0;
     const bool exch = (I.flags & GD_MC_EXCHANGE) != 0;
-    const Key key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0};
+    const Key key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, split};
     Plan &pl = plans[key];
     pl.tile = t;
+    pl.split = split;
     pl.n_stages = ns;
     pl.resident = res;
     pl.group_major = gm ? 1 : 0;
@@ -335,6 +338,7 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   R.spe = E.spe;
   R.err = E.ctx->d_err;
   R.hb_pairs = pl.hb_pairs;
+  R.split = pl.split;
   return R;
 }
 
@@ -354,7 +358,7 @@ gd_status ens_prepare(Ens &E, int n_steps) {
       pl.auto_machines = std::max(1, occ) * E.ctx->n_sm;
     }
     const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
-    if (mode == GD_SCHED_AUTO && pl.grid <= machines) continue;
+    if (pl.split > 1 || (mode == GD_SCHED_AUTO && pl.grid <= machines)) continue;
     bool have = false;
     for (const Plan::Sched &s : pl.scheds)
       have = have || (s.n_steps == n_steps && s.machines == machines);
@@ -378,6 +382,7 @@ gd_status ens_prepare(Ens &E, int n_steps) {
 const Plan::Sched *find_sched(const Ens &E, const Plan &pl, int n_steps) {
   const int mode = E.ctx->sched_mode;
   if (mode == GD_SCHED_WAVES) return nullptr;
+  if (pl.split > 1) return nullptr;  // split plans' staging is per rank: never a schedule
   const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
   if (mode == GD_SCHED_AUTO && pl.grid <= machines) return nullptr;
   for (const Plan::Sched &s : pl.scheds)
@@ -407,13 +412,14 @@ gd_status launch_plans(Ens &E, int mode, int step0, int n_steps, bool device_ste
     R.step0 = step0;
     R.n_steps = n_steps;
     R.step_ptr = device_step ? E.d_step : nullptr;
-    int grid = pl.grid;
+    int grid = pl.grid * pl.split;
     if (mode == KMODE_REMC) {
       if (const Plan::Sched *sc = find_sched(E, pl, n_steps)) {
         R.pieces = sc->d_pieces;
         R.piece_off = sc->d_off;
         R.ticket = sc->d_ticket;
         R.progress = pl.d_progress;
+        R.split = 1;
         grid = sc->grid;
       }
     }

@@ -130,6 +130,10 @@ struct KRun {
   int step0, n_steps;
   const int *step_ptr;
   int item_step;
+  int split;             // REMC / INIT without a schedule: clusters of `split`
+                         // CTAs (<= 8) share each unit, CTA rank r taking the
+                         // protein tiles r, r + split, ... (grid = units x split);
+                         // 0 or 1: one CTA per unit
   int hb_pairs;          // most atom pairs with an H-bond term in any warp of
                          // any item (hb_pairs_of); selects the kernel variant
   // Persistent schedule (REMC; nullptr: CTA b runs every step of unit b,
@@ -170,7 +174,7 @@ struct KGroup {
   int item, p, l, pad;
 };
 
-size_t dock_smem_bytes(int A, int P, int NA, int n_stages);
+size_t dock_smem_bytes(int A, int P, int NA, int n_stages, int split = 1);
 
 // Kernel launchers (gd_kernels.cu); return the launch status.
 cudaError_t launch_dock(const KRun &R, int NA, int grid, cudaStream_t s);

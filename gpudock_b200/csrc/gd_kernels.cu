@@ -78,7 +78,7 @@ static_assert(sizeof(KItem) % 8 == 0, "KItem must keep the barriers 8-byte align
 // point type pt.  Slot s = ag + A k holds ligand atom order[s].
 struct SmemLayout {
   size_t ptab, htab, hmask, slot_q, slot_t, slot_a, tiles, red, hpc, lane, item, bars, ctl,
-      total;
+      xch, xch_step, total;
 };
 
 // Piece bookkeeping of a CTA, in shared memory so that none of it holds a
@@ -100,7 +100,11 @@ struct PieceCtl {
 constexpr int MAX_PRT_KEY = 1 << 16;
 static_assert(sizeof(PieceCtl) <= 64, "PieceCtl fits its slot");
 
-__host__ __device__ inline SmemLayout smem_layout(int A, int P, int NA, int NS) {
+// split > 1: the launch runs as clusters of `split` CTAs that share a unit;
+// each CTA then also holds two (step parity) exchange buffers of its
+// per-replica partial sums: NRED FP64 terms and one FP32 hydrophobic sum per
+// atom slot, 32 lanes each.
+__host__ __device__ inline SmemLayout smem_layout(int A, int P, int NA, int NS, int split = 1) {
   SmemLayout L;
   const size_t NH = NA / 2, MAXA = (size_t)A * NA, W = (size_t)A * P;
   size_t o = 0;
@@ -133,12 +137,16 @@ __host__ __device__ inline SmemLayout smem_layout(int A, int P, int NA, int NS) 
   o = (o + 7) & ~size_t(7);
   L.bars = o;
   o += 2 * (size_t)NS * sizeof(uint64_t);
+  o = (o + 15) & ~size_t(15);
+  L.xch = o;
+  L.xch_step = (size_t)NRED * 32 * sizeof(double) + MAXA * 32 * sizeof(float);
+  if (split > 1) o += 2 * L.xch_step;
   L.total = o;
   return L;
 }
 
-size_t dock_smem_bytes(int A, int P, int NA, int n_stages) {
-  return smem_layout(A, P, NA, n_stages).total;
+size_t dock_smem_bytes(int A, int P, int NA, int n_stages, int split) {
+  return smem_layout(A, P, NA, n_stages, split).total;
 }
 
 // Hardware approximations (PTX rsqrt / rcp / ex2, flush-to-zero).
@@ -204,7 +212,7 @@ template <int MODE>
 __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneState &me,
                                          double *s_red, const float *s_hpc, const int *s_lt,
                                          int W, int P, int MAXA, int lane, int rep, bool active,
-                                         int prt_conf, int lig_conf, int step) {
+                                         int prt_conf, int lig_conf, int step, bool primary) {
   const KTables &T = I.T;
   const int lna = T.lna;
   const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
@@ -286,7 +294,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
         acc = 1;  // forced accept with beta = 0 (montecarlo_d.cu:236-239)
       } else {
         acc = metropolis(e[9], me.e_old[9], me.mbeta, u01(me.u_bits));
-        if (active && I.record && (I.rec_ring || step < I.rec_steps)) {
+        if (primary && active && I.record && (I.rec_ring || step < I.rec_steps)) {
           const int slot = I.rec_ring ? step % I.rec_steps : step;
           gd_record *rc = I.record + (size_t)rep * I.rec_steps + slot;
           rc->idx_rep = rep;
@@ -347,8 +355,10 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
             if (prob > u01(o.x)) {
               s_tmp[b + o1] = s_tmp[b + o2];
               s_tmp[b + o2] = tt;
-              atomicAdd(&I.acs_exchg[o1], 1);
-              atomicAdd(&I.acs_exchg[o2], 1);
+              if (primary) {  // once per cluster
+                atomicAdd(&I.acs_exchg[o1], 1);
+                atomicAdd(&I.acs_exchg[o2], 1);
+              }
             }
           }
         }
@@ -530,7 +540,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   extern __shared__ __align__(128) unsigned char smem[];
   const int A = R.A, P = R.P, W = A * P, NS = R.n_stages;
   const int MAXA = A * NA;
-  const SmemLayout SL = smem_layout(A, P, NA, NS);
+  // split launch: clusters of csize CTAs, rank crank, share one unit; CTA
+  // crank takes the protein tiles crank, crank + csize, ...
+  const int csize = (MODE != KMODE_POSES && !PIECES && R.split > 1) ? R.split : 1;
+  const SmemLayout SL = smem_layout(A, P, NA, NS, csize);
   float4 *s_ptab = reinterpret_cast<float4 *>(smem + SL.ptab);
   float4 *s_htab = reinterpret_cast<float4 *>(smem + SL.htab);
   uint32_t *s_hmask = reinterpret_cast<uint32_t *>(smem + SL.hmask);
@@ -577,7 +590,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   for (;;) {
   const int pc = s_ctl->pc;
   if (pc >= s_ctl->pc_end) break;
-  int unit = blockIdx.x, lo = 0, hi = -1;  // hi < 0: every step of the launch
+  int unit = blockIdx.x / csize, lo = 0, hi = -1;  // hi < 0: every step of the launch
   bool wait_dep = false;
   if (PIECES) {
     const int4 pz = R.pieces[pc];
@@ -660,6 +673,8 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     lane_rep = rep0 + (lane < n_act ? lane : 0);
   }
   const int n_tiles = (T.pnp + TILE_PTS - 1) / TILE_PTS;
+  const int crank0 = csize > 1 ? cluster_rank() : 0;
+  const int n_tl = (n_tiles - crank0 + csize - 1) / csize;  // tiles of this CTA
   const bool resident = R.resident != 0;
   const int launch_steps = (MODE != KMODE_REMC) ? 1 : (R.item_step ? I.n_run : R.n_steps);
   const int launch_base = (MODE == KMODE_REMC && R.item_step)  ? I.step0
@@ -677,7 +692,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   // the last warp to finish a stage (elected by the s_done counter) refills it.
   const float4 *src_a = T.pt_a + (size_t)prt_conf * T.pnp_pad;
   const float2 *src_b = T.pt_b;
-  const int n_seq = passes * n_tiles;
+  const int n_seq = passes * n_tl;
   auto issue_tile = [&](int s, int t) {
     unsigned char *dst = s_tiles + (size_t)s * STAGE_BYTES;
     mbar_arrive_expect_tx(&s_full[s], STAGE_BYTES);
@@ -694,9 +709,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     fence_proxy_async_smem();
     if (resident) {
       if (reload)
-        for (int t = 0; t < n_tiles; ++t) issue_tile(t, t);
+        for (int tl = 0; tl < n_tl; ++tl) issue_tile(tl, crank0 + csize * tl);
     } else {
-      for (int q = 0; q < min(NS, n_seq); ++q) issue_tile((it + q) % NS, q % n_tiles);
+      for (int q = 0; q < min(NS, n_seq); ++q)
+        issue_tile((it + q) % NS, crank0 + csize * (q % n_tl));
     }
     // the steps before this piece ran on another CTA: wait until it has
     // written their state back (bounded; code 4 if it never does)
@@ -840,13 +856,14 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     // Streaming: the same split of every tile of the ring, and every warp
     // waits for every stage and reports it done, chunk or not
     constexpr int CPT = TILE_PTS / CHUNK;  // chunks per tile
-    for (int t = 0; t < n_tiles; ++t, ++it) {
+    for (int tl = 0; tl < n_tl; ++tl, ++it) {
+      const int t = crank0 + csize * tl;  // protein tile
       const int nvalid = min(TILE_PTS, T.pnp - t * TILE_PTS);
       const int nvalid2 = nvalid;
       const int k0 = ((pg - (t * CPT) % P) % P + P) % P;
       const int kstep = P;
       if (resident && k0 * CHUNK >= nvalid2) continue;  // no chunk of this tile here
-      const int s = resident ? t : (it % NS);
+      const int s = resident ? tl : (it % NS);
       // resident tiles: the phase of their latest load (s_ctl->gen loads so far)
       const uint32_t ph = resident ? (uint32_t)((s_ctl->gen - 1) & 1) : (uint32_t)((it / NS) & 1);
       mbar_wait(&s_full[s], ph, R.err, 2);
@@ -911,7 +928,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
             const int q = it - s_ctl->first_it;  // position within the piece
             if (q + NS < n_seq) {
               fence_proxy_async_smem();
-              issue_tile(s, (q + NS) % n_tiles);
+              issue_tile(s, crank0 + csize * ((q + NS) % n_tl));
             }
           }
         }
@@ -922,7 +939,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     double dkde = 0.0, dlhm = 0.0;
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
-      if (k < n_my && k % P == pg) {
+      if (k < n_my && k % P == pg && crank0 == 0) {  // rank 0 of a split
         const int lt = s_lt[ag + A * k];
         const int kb = T.kde_off[lt], ke = T.kde_off[lt + 1];
         if (ke > kb) {
@@ -941,7 +958,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       }
     }
     // ---- LHM position restraints: MCS records m = warp, warp + W, ... -------
-    for (int m = warp; m < T.pos; m += W) {
+    for (int m = crank0 == 0 ? warp : T.pos; m < T.pos; m += W) {
       float sv = 0.f;
       const float4 *Mm = T.mcs + (size_t)m * lna;
       for (int l = 0; l < lna; ++l) {
@@ -964,15 +981,52 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       my_red[7 * 32] = dlhm;
     }
     named_sync(1, W * 32);
-    if (warp == 0)
+    if (csize > 1) {
+      // split: this CTA's partial sums go to the exchange buffer of the step's
+      // parity; after the cluster barrier every CTA adds all ranks' buffers in
+      // rank order (the same totals in every CTA) and takes the same decision.
+      // A buffer is rewritten two steps later, after the next barrier, which
+      // no CTA passes before it has read this step's buffers.
+      unsigned char *xb = smem + SL.xch + (size_t)(si & 1) * SL.xch_step;
+      double *xs = reinterpret_cast<double *>(xb);
+      float *xh = reinterpret_cast<float *>(xb + (size_t)NRED * 32 * sizeof(double));
+      if (warp == 0) {
+        for (int i = 0; i < NRED; ++i) {
+          double acc = 0.0;
+          for (int w = 0; w < W; ++w) acc += s_red[((size_t)w * NRED + i) * 32 + lane];
+          xs[i * 32 + lane] = acc;
+        }
+        for (int a = 0; a < lna; ++a) {
+          float h = 0.f;
+          for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
+          xh[a * 32 + lane] = h;
+        }
+      }
+      cluster_sync_all();
+      if (warp == 0) {
+        for (int i = 0; i < NRED; ++i) {
+          double acc = 0.0;
+          for (int r = 0; r < csize; ++r) acc += cluster_map(xs, r)[i * 32 + lane];
+          s_red[(size_t)i * 32 + lane] = acc;  // warp 0's slots
+        }
+        for (int a = 0; a < lna; ++a) {
+          float h = 0.f;
+          for (int r = 0; r < csize; ++r) h += cluster_map(xh, r)[a * 32 + lane];
+          s_hpc[(size_t)a * 32 + lane] = h;  // tile group 0's slots
+        }
+        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, MAXA, lane, rep, active, prt_conf,
+                          lig_conf, step, crank0 == 0);
+      }
+    } else if (warp == 0) {
       finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, MAXA, lane, rep, active, prt_conf,
-                        lig_conf, step);
+                        lig_conf, step, true);
+    }
     // the next step's first barrier orders warp 0's updates (and its use of
     // s_red for the exchange) before any other warp touches them again
   }
 
-  // ---- write the replica state back ----------------------------------------
-  if (MODE != KMODE_POSES && warp == 0 && active) {
+  // ---- write the replica state back (rank 0 of a split) ---------------------
+  if (MODE != KMODE_POSES && warp == 0 && active && crank0 == 0) {
 #pragma unroll
     for (int i = 0; i < 6; ++i) I.m_old[(size_t)rep * 6 + i] = me.m_old[i];
 #pragma unroll
@@ -1000,6 +1054,9 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   }
   __syncthreads();
   }  // pieces
+  // a split CTA leaves only when no other CTA of its cluster can still read
+  // its exchange buffers
+  if (csize > 1) cluster_sync_all();
 }
 
 // Temperature exchange, one thread per (item, protein conf, ligand conf)
@@ -1109,7 +1166,8 @@ __global__ void fma_peak_kernel(float *out, int iters) {
 // ---------------------------------------------------------------------------
 template <int MODE, int NA, int HB, bool PIECES>
 static cudaError_t launch_kernel(const KRun &R, int grid, cudaStream_t s, int *occ) {
-  const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages);
+  const int split = (MODE != KMODE_POSES && !PIECES && R.split > 1) ? R.split : 1;
+  const size_t smem = dock_smem_bytes(R.A, R.P, NA, R.n_stages, split);
   const int threads = R.A * R.P * 32;
   cudaError_t e = cudaFuncSetAttribute(dock_kernel<MODE, NA, HB, PIECES>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1117,8 +1175,25 @@ static cudaError_t launch_kernel(const KRun &R, int grid, cudaStream_t s, int *o
   if (occ)  // occupancy query instead of a launch
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, dock_kernel<MODE, NA, HB, PIECES>,
                                                          threads, smem);
-  dock_kernel<MODE, NA, HB, PIECES><<<grid, threads, smem, s>>>(R);
-  return cudaGetLastError();
+  if (split == 1) {
+    dock_kernel<MODE, NA, HB, PIECES><<<grid, threads, smem, s>>>(R);
+    return cudaGetLastError();
+  }
+  // clusters of `split` CTAs (grid = units x split), on SMs of one GPC
+  if (split > 8 || grid % split) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = split;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, dock_kernel<MODE, NA, HB, PIECES>, R);
 }
 
 template <int MODE, int NA, int HB>

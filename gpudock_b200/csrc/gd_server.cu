@@ -91,6 +91,7 @@ struct Req {
 struct Lane {
   Tile tile;
   int ns = 0, res = 0, gm = 0, spe = 0;
+  int split = 1;                    // CTAs (a cluster) per request unit
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   int *d_err = nullptr;             // the lane's kernel error word
@@ -106,7 +107,7 @@ struct Lane {
   size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
 };
 
-using LaneKey = std::tuple<int, int, int, int, int, int, int>;
+using LaneKey = std::tuple<int, int, int, int, int, int, int, int>;
 constexpr int kMaxLanes = 256;
 
 }  // namespace
@@ -193,11 +194,12 @@ gd_status grow(T **p, size_t *cap, size_t need, cudaStream_t s) {
 gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   const KTables &T = r->dcx->T;
   Tile t = tile_for(S->ctx, T);
+  const int split = split_for(S->ctx, T);
   int ns, res;
-  pick_stages(T, t, &ns, &res);
+  pick_stages(T, t, &ns, &res, split);
   const bool gm = (32 % r->mc.n_tmp) == 0;
   const int spe = r->mc.steps_per_exchange;
-  const LaneKey key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe};
+  const LaneKey key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe, split};
   auto it = S->lanes.find(key);
   if (it != S->lanes.end()) {
     *out = it->second.get();
@@ -209,6 +211,7 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   L->res = res;
   L->gm = gm ? 1 : 0;
   L->spe = spe;
+  L->split = split;
   const int slot = (int)S->lanes.size();
   if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d launch shapes in the server", kMaxLanes);
   GD_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
@@ -264,7 +267,8 @@ gd_status admit(gd_server *S, Req *r) {
   I.idx_tmp = r->d_idx;
   I.acs_mc = r->d_acs;
   r->step = 0;
-  r->cost = (double)lna_bucket(I.T.lna) * I.T.pnp;
+  // time per MC step: the unit's pairs over the CTAs that share them
+  r->cost = (double)lna_bucket(I.T.lna) * I.T.pnp / r->lane->split;
   return GD_OK;
 }
 
@@ -341,8 +345,9 @@ gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int m
   R.n_steps = 0;  // per item (item_step)
   R.item_step = 1;
   R.err = L.d_err;
+  R.split = L.split;
   for (const Req *r : rs) R.hb_pairs = std::max(R.hb_pairs, hb_pairs_of(r->item.T, L.tile.A));
-  GD_CUDA(launch_dock(R, L.tile.NA, (int)n_cta, s));
+  GD_CUDA(launch_dock(R, L.tile.NA, (int)n_cta * L.split, s));
   S->ctx->launches += 1;
   S->n_launch += 1;
   if (!groups.empty()) {

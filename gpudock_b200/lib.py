@@ -44,6 +44,7 @@ def _declare(lib):
         "gd_autotune": ([P, P, C.POINTER(abi.GdTile), C.POINTER(C.c_double)], i32),
         "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
         "gd_ctx_set_schedule": ([P, i32, i32], i32),
+        "gd_ctx_set_split": ([P, i32], i32),
         "gd_load": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                      C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara), C.c_uint,
                      C.POINTER(P)], i32),
@@ -163,6 +164,10 @@ class Context:
     @property
     def launches(self) -> int:
         return int(self._lib.gd_ctx_launch_count(self.h))
+
+    def set_split(self, split: int):
+        """CTAs per 32-replica unit of MC launches (0: chosen per complex)."""
+        check(self._lib.gd_ctx_set_split(self.h, split), "gd_ctx_set_split")
 
     def set_schedule(self, mode: int, machines: int = 0):
         """abi.SCHED_AUTO / SCHED_WAVES / SCHED_PERSISTENT (over `machines` CTAs)."""

@@ -306,6 +306,21 @@ gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile);
 enum { GD_SCHED_AUTO = 0, GD_SCHED_WAVES = 1, GD_SCHED_PERSISTENT = 2 };
 gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
 
+/* How many CTAs share each 32-replica unit of an MC launch.  With split > 1
+ * the unit runs on a thread-block cluster of `split` CTAs (SMs of one GPC):
+ * CTA r evaluates the protein tiles r, r + split, ..., the CTAs add their
+ * partial energies through distributed shared memory every MC step (in
+ * rank order) and all take the same decision.  A complex's run then takes
+ * about 1/split of the time when SMs are free (latency), at a few percent
+ * more total work.  split = 0 (the default) chooses per complex from its
+ * size alone: the largest power of two <= ligand-size bucket x protein
+ * points / 150,000, at most 8 (a 40-atom ligand against 4,000 points runs
+ * unsplit, 120 atoms against 10,000 points on 8 CTAs); 1, 2, 4 or 8 fix it
+ * for every complex.  A run's results depend on its split (the partial sums
+ * are added in another order) but never on what runs beside it.  Applies to
+ * runs, batches and server lanes created after the call. */
+gd_status gd_ctx_set_split(gd_ctx *ctx, int split);
+
 /* ------------------------------------------------------------------------ */
 /* Pose energies (CalcEnergy_d after Move_d on a given move vector)         */
 /* ------------------------------------------------------------------------ */
