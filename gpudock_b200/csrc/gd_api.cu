@@ -83,13 +83,23 @@ void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident, 
 
 int lna_bucket(int lna) { return std::min(((lna + 7) / 8) * 8, MAX_LNA); }
 
-int split_for(gd_ctx *ctx, const KTables &T) {
+int split_for(gd_ctx *ctx, const KTables &T, int run_units) {
   if (ctx->split_mode > 0) return ctx->split_mode;
-  // the largest power of two <= cost / kSplitCost, at most 8
+  // the largest power of two <= cost / kSplitCost and <= SMs / units, at
+  // most 8: a run that fills the GPU with units gains nothing from splitting
   const double cost = (double)lna_bucket(T.lna) * T.pnp;
+  const int free = ctx->n_sm / std::max(1, run_units);
   int k = 1;
-  while (k < 8 && cost >= kSplitCost * 2.0 * k) k *= 2;
+  while (k < 8 && cost >= kSplitCost * 2.0 * k && 2 * k <= free) k *= 2;
   return k;
+}
+
+int units_of(int n_prt, int n_lig, int n_tmp) {
+  if (32 % n_tmp == 0) {
+    const int G = 32 / n_tmp;  // ligand conformations per unit
+    return n_prt * ((n_lig + G - 1) / G);
+  }
+  return n_prt * ((n_lig * n_tmp + 31) / 32);
 }
 
 Tile tile_for(gd_ctx *ctx, const KTables &T) {

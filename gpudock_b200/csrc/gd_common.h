@@ -102,10 +102,15 @@ gd_status kernel_error(int code);
 int lna_bucket(int lna);
 Tile tile_for(gd_ctx *ctx, const KTables &T);
 // CTAs (a thread-block cluster) that share each 32-replica unit of a complex
-// in MC launches: a function of the complex alone (ligand-size bucket x
-// protein points), so its runs are the same in any mix; 1 below 2 kSplitCost.
-constexpr double kSplitCost = 150000.0;
-int split_for(gd_ctx *ctx, const KTables &T);
+// in MC launches: a function of the complex (ligand-size bucket x protein
+// points) and of the units of its own run (a server request is a run of its
+// own), never of what else runs, so results are the same in any mix.  The
+// largest power of two <= cost / kSplitCost and <= SMs / units, at most 8.
+constexpr double kSplitCost = 85000.0;
+int split_for(gd_ctx *ctx, const KTables &T, int run_units);
+// 32-replica units of a complex's replicas (n_prt x n_lig x n_tmp): whole
+// exchange groups per unit when n_tmp divides 32.
+int units_of(int n_prt, int n_lig, int n_tmp);
 
 // Launches of different shapes (one per launch plan) are independent; each
 // kernel holds one CTA per SM, so a plan with fewer CTAs than SMs leaves the

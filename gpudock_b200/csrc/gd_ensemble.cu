@@ -247,10 +247,12 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
   std::map<Key, std::vector<std::tuple<double, int, int, int>>> ctas;  // cost, item, rep0, n
   std::map<Key, Plan> plans;
   std::vector<KGroup> groups;
+  int run_units = 0;  // units of the whole run (the split rule's bound)
+  for (const KItem &I : E.items) run_units += units_of(I.n_prt, I.n_lig_conf, I.n_tmp);
   for (int i = 0; i < n; ++i) {
     const KItem &I = E.items[i];
     Tile t = tile_for(ctx, I.T);
-    const int split = split_for(ctx, I.T);
+    const int split = split_for(ctx, I.T, run_units);
     int ns, res;
     pick_stages(I.T, t, &ns, &res, split);
     const int nt = I.n_tmp, nl = I.n_lig_conf;

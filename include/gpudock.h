@@ -313,12 +313,15 @@ gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
  * rank order) and all take the same decision.  A complex's run then takes
  * about 1/split of the time when SMs are free (latency), at a few percent
  * more total work.  split = 0 (the default) chooses per complex from its
- * size alone: the largest power of two <= ligand-size bucket x protein
- * points / 150,000, at most 8 (a 40-atom ligand against 4,000 points runs
- * unsplit, 120 atoms against 10,000 points on 8 CTAs); 1, 2, 4 or 8 fix it
- * for every complex.  A run's results depend on its split (the partial sums
- * are added in another order) but never on what runs beside it.  Applies to
- * runs, batches and server lanes created after the call. */
+ * size and its own run: the largest power of two <= ligand-size bucket x
+ * protein points / 85,000 and <= SMs / units of the run, at most 8 (a
+ * 40-atom ligand against 4,000 points runs unsplit; a served request of 32
+ * replicas with 120 atoms against 10,000 points runs on 8 CTAs; a batch
+ * or ensemble with more units than SMs runs unsplit); 1, 2, 4 or 8 fix it
+ * for every complex.  A server request is a run of its own.  A run's
+ * results depend on its split (the partial sums are added in another
+ * order) but never on what runs beside it.  Applies to runs, batches and
+ * server lanes created after the call. */
 gd_status gd_ctx_set_split(gd_ctx *ctx, int split);
 
 /* ------------------------------------------------------------------------ */

@@ -103,7 +103,7 @@ def test_split_batch_equals_alone():
 
 
 def test_split_default_rule_and_server():
-    """A 100-atom ligand against 8,000 points splits 4 ways by default; served
+    """A 100-atom ligand against 8,000 points splits 8 ways by default; served
     alone, served among smaller requests and run in the plain form it gives
     the same trajectory."""
     raw, _, _ = synth.default_ff()
