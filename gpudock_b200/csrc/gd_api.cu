@@ -83,14 +83,14 @@ void pick_stages(const KTables &T, const Tile &t, int *n_stages, int *resident, 
 
 int lna_bucket(int lna) { return std::min(((lna + 7) / 8) * 8, MAX_LNA); }
 
-int split_for(gd_ctx *ctx, const KTables &T, int run_units) {
+int split_for(gd_ctx *ctx, const KTables &T, int run_units, double min_cost) {
   if (ctx->split_mode > 0) return ctx->split_mode;
-  // the largest power of two <= cost / kSplitCost and <= SMs / units, at
-  // most 8: a run that fills the GPU with units gains nothing from splitting
+  // the largest power of two <= cost / min_cost and <= SMs / units, at most
+  // 8: a run that fills the GPU with units gains nothing from splitting
   const double cost = (double)lna_bucket(T.lna) * T.pnp;
   const int free = ctx->n_sm / std::max(1, run_units);
   int k = 1;
-  while (k < 8 && cost >= kSplitCost * 2.0 * k && 2 * k <= free) k *= 2;
+  while (k < 8 && cost >= min_cost * 2.0 * k && 2 * k <= free) k *= 2;
   return k;
 }
 

@@ -103,11 +103,15 @@ int lna_bucket(int lna);
 Tile tile_for(gd_ctx *ctx, const KTables &T);
 // CTAs (a thread-block cluster) that share each 32-replica unit of a complex
 // in MC launches: a function of the complex (ligand-size bucket x protein
-// points) and of the units of its own run (a server request is a run of its
-// own), never of what else runs, so results are the same in any mix.  The
-// largest power of two <= cost / kSplitCost and <= SMs / units, at most 8.
-constexpr double kSplitCost = 85000.0;
-int split_for(gd_ctx *ctx, const KTables &T, int run_units);
+// points) and of the units of its own run, never of what else runs, so
+// results are the same in any mix.  The largest power of two <= cost /
+// min_cost and <= SMs / units, at most 8.  Runs (gd_remc, gd_batch) have the
+// GPU to themselves and split down to kRunSplitCost pairs per CTA; a server
+// request is a run of its own among others and splits only from
+// kServeSplitCost, so that splitting under load costs little throughput.
+constexpr double kRunSplitCost = 4500.0;
+constexpr double kServeSplitCost = 85000.0;
+int split_for(gd_ctx *ctx, const KTables &T, int run_units, double min_cost);
 // 32-replica units of a complex's replicas (n_prt x n_lig x n_tmp): whole
 // exchange groups per unit when n_tmp divides 32.
 int units_of(int n_prt, int n_lig, int n_tmp);

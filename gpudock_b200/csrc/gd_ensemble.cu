@@ -252,7 +252,7 @@ gd_status ens_build(Ens &E, gd_ctx *ctx, int n, const gd_dcomplex *const *dcx,
   for (int i = 0; i < n; ++i) {
     const KItem &I = E.items[i];
     Tile t = tile_for(ctx, I.T);
-    const int split = split_for(ctx, I.T, run_units);
+    const int split = split_for(ctx, I.T, run_units, kRunSplitCost);
     int ns, res;
     pick_stages(I.T, t, &ns, &res, split);
     const int nt = I.n_tmp, nl = I.n_lig_conf;

@@ -195,7 +195,8 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   const KTables &T = r->dcx->T;
   Tile t = tile_for(S->ctx, T);
   // a request is a run of its own
-  const int split = split_for(S->ctx, T, units_of(T.n_prt, T.n_lig, r->mc.n_tmp));
+  const int split =
+      split_for(S->ctx, T, units_of(T.n_prt, T.n_lig, r->mc.n_tmp), kServeSplitCost);
   int ns, res;
   pick_stages(T, t, &ns, &res, split);
   const bool gm = (32 % r->mc.n_tmp) == 0;

@@ -314,11 +314,13 @@ gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
  * about 1/split of the time when SMs are free (latency), at a few percent
  * more total work.  split = 0 (the default) chooses per complex from its
  * size and its own run: the largest power of two <= ligand-size bucket x
- * protein points / 85,000 and <= SMs / units of the run, at most 8 (a
- * 40-atom ligand against 4,000 points runs unsplit; a served request of 32
- * replicas with 120 atoms against 10,000 points runs on 8 CTAs; a batch
- * or ensemble with more units than SMs runs unsplit); 1, 2, 4 or 8 fix it
- * for every complex.  A server request is a run of its own.  A run's
+ * protein points / c and <= SMs / units of the run, at most 8, with
+ * c = 4,500 for runs and batches (they have the GPU to themselves: a
+ * 24-atom ligand against 1,500 points runs on 8 CTAs, an ensemble or batch
+ * with more units than SMs unsplit) and c = 85,000 for server requests
+ * (each a run of its own among others, so that splitting under load costs
+ * little throughput: 120 atoms against 10,000 points on 8 CTAs, 30 atoms
+ * against 4,000 unsplit); 1, 2, 4 or 8 fix it for every complex.  A run's
  * results depend on its split (the partial sums are added in another
  * order) but never on what runs beside it.  Applies to runs, batches and
  * server lanes created after the call. */

@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def ctx():
     c = lib.Context(0)
+    c.set_split(1)  # persistent schedules are for unsplit units
     yield c
     c.set_schedule(abi.SCHED_AUTO)
     c.close()

@@ -22,8 +22,11 @@ def _protein_and_ligands(pnp, lnas, seed, n_prt=1):
     return cxs
 
 
-def _run_alone(cx, steps, spe, mb, seed, stream):
+def _run_alone(cx, steps, spe, mb, seed, stream, split=1):
+    """The plain-form run of a complex with the split its server request gets
+    (these requests are below the server's split threshold: unsplit)."""
     ctx = lib.Context(0)
+    ctx.set_split(split)
     d = lib.DeviceComplex(ctx, cx)
     r = lib.Remc(d, steps, spe, mb, seed=seed, stream_id=stream,
                  flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY)
