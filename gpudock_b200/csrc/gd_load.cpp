@@ -77,10 +77,30 @@ const SidePoints kSide[GD_NRES] = {
     {1, {23, 0}, {2, 0}},  {1, {17, 0}, {2, 0}},  {2, {28, 29}, {2, 3}}, {1, {25, 0}, {2, 0}},
 };
 
+// getPntCode (data.C:391-460): protein effective-point names, index = code.
+const char *const kPntNames[GD_NPT] = {"CA", "PP", "A1", "C1", "D1", "E1", "E2", "F1",
+                                       "F2", "H1", "H2", "I1", "K1", "K2", "L1", "M1",
+                                       "M2", "N1", "P1", "Q1", "Q2", "R1", "R2", "S1",
+                                       "T1", "V1", "W1", "W2", "Y1", "Y2"};
+// getResCodeOne (data.C:290-336): one-letter residue codes, index = code.
+const char kResOne[GD_NRES + 1] = "ARCPLIEHWTMDGFKQSNYV";
+
 int lig_code(const std::string &s) {
   for (int i = 0; i < GD_NLT; ++i)
     if (s == kLigNames[i]) return i;
   return kBadType;
+}
+
+int pnt_code(const std::string &s) {
+  for (int i = 0; i < GD_NPT; ++i)
+    if (s == kPntNames[i]) return i;
+  return -1;
+}
+
+int res_one_code(const std::string &s) {
+  if (s.size() != 1) return -1;
+  const char *p = std::strchr(kResOne, s[0]);
+  return (p && *p) ? (int)(p - kResOne) : -1;
 }
 
 int res_code(const std::string &s) {
@@ -475,7 +495,116 @@ gd_status load_lhm(const char *path, const char *ligand_id, gd_loaded *L) {
   return GD_OK;
 }
 
+// The force-field parameter file (loadEnePara, load.C:1139-1324): tagged
+// lines of whitespace-separated fields, values by atof stored as floats, a
+// missing field reading as 0.  Unknown point, ligand or residue names are
+// errors (the reference exits on the first and the third and indexes past
+// its tables with the second).  Afterwards the residue hydrophobicities are
+// rescaled to [-1, 1]: difference and quotient in float, "* 2 - 1" in
+// double, clamped (load.C:1297-1323).
+gd_status load_ff_params(const char *path, gd_enepara_raw *R) {
+  std::vector<std::string> lines;
+  if (!read_lines(path, &lines)) return fail(GD_EIO, "cannot open %s", path);
+  for (size_t li = 0; li < lines.size(); ++li) {
+    const std::string &line = lines[li];
+    if (line.size() <= 3) continue;
+    const std::string tag = line.substr(0, 3);
+    const std::vector<std::string> w = tokens(line);
+    auto val = [&](size_t k) { return k < w.size() ? fnum(w[k]) : 0.0f; };
+    auto name = [&](size_t k) { return k < w.size() ? w[k] : std::string(); };
+    auto bad = [&](const char *what) {
+      return fail(GD_EINVAL, "%s line %zu: unknown %s", path, li + 1, what);
+    };
+    if (tag == "VDW" || tag == "PMF" || tag == "HDB") {
+      const int p = pnt_code(name(1)), l = lig_code(name(2));
+      if (p < 0) return bad("point type");
+      if (l >= GD_NLT) return bad("ligand type");
+      float(*t)[GD_NLT][2] = tag == "VDW" ? R->vdw : tag == "PMF" ? R->pmf : R->hdb;
+      t[p][l][0] = val(3);
+      t[p][l][1] = val(4);
+    } else if (tag == "PLJ") {
+      for (int k = 0; k < 3; ++k) R->lj[k] = val(1 + k);
+    } else if (tag == "ELE") {
+      // "<res>C": the residue's backbone class (ele[30 + residue]), else a
+      // point type
+      const std::string n = name(1);
+      if (n.size() >= 2 && n[1] == 'C') {
+        const int r = res_one_code(n.substr(0, 1));
+        if (r < 0) return bad("residue");
+        R->ele[GD_NPT + r] = val(2);
+      } else {
+        const int p = pnt_code(n);
+        if (p < 0) return bad("point type");
+        R->ele[p] = val(2);
+      }
+    } else if (tag == "PEL") {
+      for (int k = 0; k < 2; ++k) R->el[k] = val(1 + k);
+    } else if (tag == "HPP") {
+      const int r = res_one_code(name(1));
+      if (r < 0) return bad("residue");
+      R->hpp[r] = val(2);
+    } else if (tag == "HPL") {
+      const int l = lig_code(name(1));
+      if (l >= GD_NLT) return bad("ligand type");
+      R->hpl[l][0] = val(2);
+      R->hpl[l][1] = val(3);
+    } else if (tag == "WEI") {
+      for (int k = 0; k < GD_NTERM; ++k) R->w[k] = val(1 + k);
+    } else if (tag == "KDE") {
+      R->kde = val(1);
+    }
+  }
+  float lo = 1e6f, hi = -1e6f;
+  for (int r = 0; r < GD_NRES; ++r) {
+    lo = std::min(lo, R->hpp[r]);
+    hi = std::max(hi, R->hpp[r]);
+  }
+  for (int r = 0; r < GD_NRES; ++r) {
+    const float q = (R->hpp[r] - lo) / (hi - lo);
+    float h = (float)((double)q * 2.0 - 1.0);
+    if (h < -1.0f) h = -1.0f;
+    if (h > 1.0f) h = 1.0f;
+    R->hpp[r] = h;
+  }
+  return GD_OK;
+}
+
+// One value per line from its first 30 characters, read as a float by a
+// stream (which leaves 0 where no number parses and the largest float on
+// overflow), for the first GD_NTERM lines: loadWeight and loadNorPara
+// (load.C:1326-1419).  Later lines are ignored (the reference writes them
+// past its arrays).
+gd_status load_column(const char *path, float *dst) {
+  std::vector<std::string> lines;
+  if (!read_lines(path, &lines)) return fail(GD_EIO, "cannot open %s", path);
+  for (size_t i = 0; i < lines.size() && i < (size_t)GD_NTERM; ++i) {
+    std::istringstream in(col(lines[i], 0, 30));
+    float v = 0.0f;
+    in >> v;
+    dst[i] = v;
+  }
+  return GD_OK;
+}
+
 }  // namespace
+
+extern "C" gd_status gd_load_enepara(const char *ff, const char *weights, const char *nor_a,
+                                     const char *nor_b, gd_enepara_raw *out) {
+  if (!ff || !out) return fail(GD_EINVAL, "gd_load_enepara: NULL argument");
+  gd_enepara_raw R;
+  std::memset(&R, 0, sizeof(R));
+  gd_status st;
+  try {
+    st = load_ff_params(ff, &R);
+    if (st == GD_OK && weights) st = load_column(weights, R.w);
+    if (st == GD_OK && nor_a) st = load_column(nor_a, R.a_para);
+    if (st == GD_OK && nor_b) st = load_column(nor_b, R.b_para);
+  } catch (const std::bad_alloc &) {
+    st = fail(GD_ENOMEM, "host allocation");
+  }
+  if (st == GD_OK) *out = R;
+  return st;
+}
 
 extern "C" gd_status gd_load(const char *pdb, const char *sdf, const char *lhm,
                              const char *ligand_id, const char *molid,

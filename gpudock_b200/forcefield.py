@@ -13,6 +13,7 @@ normalisation, converted by ``data/make_ff.py``.
 from __future__ import annotations
 
 import os
+import re
 
 import numpy as np
 
@@ -69,15 +70,25 @@ def empty_raw() -> dict:
     }
 
 
+_NUM = re.compile(r"\s*[+-]?(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?")
+
+
+def _atof(s: str) -> np.float32:
+    """atof stored as a float: the longest leading decimal number, else 0."""
+    m = _NUM.match(s)
+    return np.float32(float(m.group(0)) if m else 0.0)
+
+
 def parse_ff_text(text: str, raw: dict | None = None) -> dict:
     """Parses the .ff parameter format (VDW/PLJ/ELE/PEL/PMF/HPP/HPL/HDB/WEI/KDE
     lines) the way loadEnePara does, including the HPP rescaling."""
     raw = empty_raw() if raw is None else raw
-    f = np.float32
     for line in text.splitlines():
         if len(line) <= 3:
             continue
         tag, tok = line[:3], line.split()
+        tok += [""] * (abi.NTERM + 1 - len(tok))  # a missing field reads as 0
+        f = _atof
         if tag == "VDW":
             raw["vdw"][PNT_CODE[tok[1]], LIG_CODE[tok[2]]] = (f(tok[3]), f(tok[4]))
         elif tag == "PLJ":
@@ -99,8 +110,7 @@ def parse_ff_text(text: str, raw: dict | None = None) -> dict:
         elif tag == "HDB":
             raw["hdb"][PNT_CODE[tok[1]], LIG_CODE[tok[2]]] = (f(tok[3]), f(tok[4]))
         elif tag == "WEI":
-            vals = [f(v) for v in tok[1:]]
-            raw["w"][: len(vals)] = vals
+            raw["w"][:] = [f(v) for v in tok[1:abi.NTERM + 1]]
         elif tag == "KDE":
             raw["kde"][0] = f(tok[1])
     # rescale hydrophobicity to [-1, 1] (load.C:1297-1323): the difference and

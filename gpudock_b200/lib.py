@@ -51,6 +51,8 @@ def _declare(lib):
         "gd_loaded_complex": ([P, C.POINTER(abi.GdComplex)], i32),
         "gd_loaded_ligand_id": ([P], C.c_char_p),
         "gd_loaded_free": ([P], i32),
+        "gd_load_enepara": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                             C.POINTER(abi.GdEneparaRaw)], i32),
         "gd_schedule_pieces": ([C.POINTER(C.c_double), C.POINTER(C.c_int), i32, i32,
                                 C.POINTER(C.c_int), i32, C.POINTER(C.c_int),
                                 C.POINTER(C.c_int)], i32),
@@ -562,6 +564,18 @@ def read_trajectory(directory: str, stem: str):
 
 
 LOAD_PEPTIDE_ALL_MODELS = 0x1
+
+
+def load_enepara(ff: str, weights: str | None = None, nor_a: str | None = None,
+                 nor_b: str | None = None) -> abi.GdEneparaRaw:
+    """The raw force field from the reference's parameter files
+    (gd_load_enepara: loadEnePara, loadWeight, loadNorPara)."""
+    lib = load()
+    raw = abi.GdEneparaRaw()
+    enc = (lambda v: None if v is None else os.fsencode(v))
+    check(lib.gd_load_enepara(enc(ff), enc(weights), enc(nor_a), enc(nor_b), C.byref(raw)),
+          "gd_load_enepara")
+    return raw
 
 
 def load_files(pdb: str, sdf: str, lhm: str, ligand_id: str, molid: str = "MOLID",

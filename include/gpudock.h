@@ -236,6 +236,24 @@ gd_status gd_loaded_complex(const gd_loaded *loaded, gd_complex *out);
 const char *gd_loaded_ligand_id(const gd_loaded *loaded);
 gd_status gd_loaded_free(gd_loaded *loaded);
 
+/* The force-field parameter files into the raw table, as loadEnePara,
+ * loadWeight and loadNorPara (load.C:1139-1419) fill EnePara0:
+ *  ff:      tagged lines VDW / PMF / HDB <point> <ligand type> <a> <b>,
+ *           ELE <point or residue letter + "C"> <v>, HPP <residue letter>
+ *           <v>, HPL <ligand type> <a> <b>, PLJ (3 values), PEL (2), WEI
+ *           (up to 10 weights), KDE (bandwidth); other lines are skipped,
+ *           missing values read as 0, and the residue hydrophobicities are
+ *           rescaled to [-1, 1] afterwards.
+ *  weights, nor_a, nor_b: one value per line (first 30 characters) for the
+ *           term weights w and the normalisation a_para / b_para, the first
+ *           GD_NTERM lines; NULL keeps w from the WEI line and a_para /
+ *           b_para at 0.
+ * Every entry no line sets is 0.  Unreadable files give GD_EIO; unknown
+ * point, ligand or residue names give GD_EINVAL (the reference exits or
+ * indexes past its tables).  *out is written only on success. */
+gd_status gd_load_enepara(const char *ff, const char *weights, const char *nor_a,
+                          const char *nor_b, gd_enepara_raw *out);
+
 /* ------------------------------------------------------------------------ */
 /* Device context and device-resident complexes                             */
 /* ------------------------------------------------------------------------ */

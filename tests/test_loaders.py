@@ -231,3 +231,84 @@ def test_loader_errors(tmp_path):
     assert e.value.status == abi.GD_EINVAL and "unknown residue" in str(e.value)
     cx = lib.load_files(*args, raw=raw)
     assert cx.n_lig == 1 and cx.pnp > 0
+
+
+# ---------------------------------------------------------------------------
+# force-field parameter files (gd_load_enepara)
+# ---------------------------------------------------------------------------
+PARAM_FILES = {  # the parameter files each golden fixture was dumped with
+    "rem": ("gpudocksm-rem-1.2/test", "gpudocksm.ff", "08ff_opt", "08_nor_a", "08_nor_b"),
+    "smg": ("SimilarityMatirxGen/data/parameters", "paras", "08ff_opt", "08_nor_a", "08_nor_b"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PARAM_FILES))
+def test_enepara_files_match_reference_loaders(name):
+    d, *files = PARAM_FILES[name]
+    base = os.path.join(REF, d)
+    if not os.path.isdir(base):
+        pytest.skip("reference checkout not present")
+    _, _, z = load_complex(name)
+    raw = lib.load_enepara(*[os.path.join(base, f) for f in files])
+    assert bytes(raw) == z["enepara_raw"].tobytes()
+    if name == "rem":  # the packaged parameter set is these files
+        assert bytes(raw) == bytes(forcefield.raw_struct(forcefield.load_raw()))
+
+
+def test_enepara_hand_written(tmp_path):
+    ff = ["VDW CA C.3 1.5 0.25", "PMF Y2 S.O2 4.0", "HDB N1 O.2 2.9 0.7",
+          "ELE CA 0.5", "ELE KC -1.25", "HPP A 1.8", "HPP R -4.5", "HPP G -0.4",
+          "HPL C.ar 0.3 2.5", "PLJ 1 2 3", "PEL 2.0 0.5", "WEI 1 2 3", "KDE 0.25",
+          "XYZ ignored line", "VDW", ""]
+    (tmp_path / "p.ff").write_text("\n".join(ff) + "\n")
+    (tmp_path / "w").write_text("0.5\n\n2.5   trailing text\n")
+    (tmp_path / "a").write_text("\n".join(str(v) for v in range(12)) + "\n")
+    raw = lib.load_enepara(str(tmp_path / "p.ff"))
+    nlt = forcefield.LIG_CODE
+    npt = forcefield.PNT_CODE
+    assert raw.vdw[npt["CA"]][nlt["C.3"]][0] == np.float32(1.5)
+    assert raw.vdw[npt["CA"]][nlt["C.3"]][1] == np.float32(0.25)
+    assert raw.pmf[npt["Y2"]][nlt["S.O2"]][0] == np.float32(4.0)
+    assert raw.pmf[npt["Y2"]][nlt["S.O2"]][1] == 0.0  # missing value
+    assert raw.hdb[npt["N1"]][nlt["O.2"]][1] == np.float32(0.7)
+    assert raw.ele[npt["CA"]] == np.float32(0.5)
+    assert raw.ele[30 + forcefield.RES_CODE_ONE["K"]] == np.float32(-1.25)
+    # hydrophobicity rescaled over all 20 residues (unset ones are 0):
+    # min -4.5 -> -1, max 1.8 -> 1
+    hpp = np.array(raw.hpp[:], np.float32)
+    assert hpp[forcefield.RES_CODE_ONE["A"]] == 1.0 and hpp[forcefield.RES_CODE_ONE["R"]] == -1.0
+    lo, hi = np.float32(-4.5), np.float32(1.8)
+    want_g = np.float32(np.float64((np.float32(-0.4) - lo) / np.float32(hi - lo)) * 2.0 - 1.0)
+    assert hpp[forcefield.RES_CODE_ONE["G"]] == want_g
+    assert list(raw.lj) == [1.0, 2.0, 3.0] and list(raw.el) == [2.0, 0.5]
+    assert list(raw.w) == [1.0, 2.0, 3.0] + [0.0] * 7 and raw.kde == np.float32(0.25)
+    assert list(raw.a_para) == [0.0] * 10 and list(raw.b_para) == [0.0] * 10
+    # the same text through the Python parser gives the same table
+    py = forcefield.raw_struct(forcefield.parse_ff_text("\n".join(ff)))
+    assert bytes(py) == bytes(raw)
+    # weight and normalisation columns: first 30 characters of each of the
+    # first 10 lines, empty lines 0; w replaces the WEI values line by line
+    raw2 = lib.load_enepara(str(tmp_path / "p.ff"), str(tmp_path / "w"), str(tmp_path / "a"),
+                            str(tmp_path / "a"))
+    assert list(raw2.w) == [0.5, 0.0, 2.5] + [0.0] * 7
+    assert list(raw2.a_para) == [float(v) for v in range(10)]
+    assert list(raw2.b_para) == list(raw2.a_para)
+
+
+@pytest.mark.parametrize("line", ["VDW XX C.3 1 1", "PMF CA Q.9 1 1", "HPL Zz 1 1",
+                                  "ELE ZC 1", "ELE Q 1", "HPP B 1"])
+def test_enepara_unknown_names(tmp_path, line):
+    (tmp_path / "p.ff").write_text("PLJ 1 2 3\n" + line + "\n")
+    with pytest.raises(lib.GdError) as e:
+        lib.load_enepara(str(tmp_path / "p.ff"))
+    assert e.value.status == abi.GD_EINVAL
+
+
+def test_enepara_missing_files(tmp_path):
+    (tmp_path / "p.ff").write_text("PLJ 1 2 3\n")
+    for args in ([str(tmp_path / "none.ff")],
+                 [str(tmp_path / "p.ff"), str(tmp_path / "none")],
+                 [str(tmp_path / "p.ff"), None, None, str(tmp_path / "none")]):
+        with pytest.raises(lib.GdError) as e:
+            lib.load_enepara(*args)
+        assert e.value.status == abi.GD_EIO
