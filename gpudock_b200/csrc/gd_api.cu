@@ -277,6 +277,43 @@ extern "C" gd_status gd_set_temperature(int n, float floor_t, float ceil_t, floa
   return GD_OK;
 }
 
+// Rigid poses given as a translation and a rotation quaternion, as the
+// move vectors of Move_d (move_d.cu:90-105): R = Rz(m3) Ry(m4) Rx(m5), so
+// r00 = cos m3 cos m4, r10 = sin m3 cos m4, r20 = -sin m4, r21 = cos m4 sin m5,
+// r22 = cos m4 cos m5.  Where cos m4 vanishes only m5 - m3 (m4 = pi/2) or
+// m5 + m3 (m4 = -pi/2) is fixed; m3 = 0 then.  Double precision throughout.
+extern "C" gd_status gd_poses_from_quaternions(int n_pose, const float *quat_poses,
+                                               float *poses) {
+  if (n_pose < 0 || (n_pose > 0 && (!quat_poses || !poses)))
+    return fail(GD_EINVAL, "gd_poses_from_quaternions: n_pose=%d", n_pose);
+  for (int i = 0; i < n_pose; ++i) {
+    const float *q = quat_poses + (size_t)i * 7;
+    for (int k = 0; k < 7; ++k)
+      if (!std::isfinite(q[k])) return fail(GD_EINVAL, "pose %d: non-finite value", i);
+    double w = q[3], x = q[4], y = q[5], z = q[6];
+    const double nrm = std::sqrt(w * w + x * x + y * y + z * z);
+    if (!(nrm > 0.0)) return fail(GD_EINVAL, "pose %d: zero quaternion", i);
+    w /= nrm, x /= nrm, y /= nrm, z /= nrm;
+    const double r00 = 1.0 - 2.0 * (y * y + z * z), r01 = 2.0 * (x * y - w * z);
+    const double r10 = 2.0 * (x * y + w * z), r11 = 1.0 - 2.0 * (x * x + z * z);
+    const double r20 = 2.0 * (x * z - w * y), r21 = 2.0 * (y * z + w * x);
+    const double r22 = 1.0 - 2.0 * (x * x + y * y);
+    const double m4 = -std::asin(std::min(1.0, std::max(-1.0, r20)));
+    double m3, m5;
+    if (std::hypot(r00, r10) > 1e-9) {
+      m3 = std::atan2(r10, r00);
+      m5 = std::atan2(r21, r22);
+    } else {
+      m3 = 0.0;
+      m5 = r20 < 0.0 ? std::atan2(r01, r11) : std::atan2(-r01, r11);
+    }
+    float *m = poses + (size_t)i * 6;
+    m[0] = q[0], m[1] = q[1], m[2] = q[2];
+    m[3] = (float)m3, m[4] = (float)m4, m[5] = (float)m5;
+  }
+  return GD_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Validation
 // ---------------------------------------------------------------------------

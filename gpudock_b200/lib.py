@@ -33,6 +33,7 @@ def _declare(lib):
         "gd_version": ([], C.c_char_p),
         "gd_enepara_optimize": ([C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara)], i32),
         "gd_set_temperature": ([i32, C.c_float, C.c_float, abi.f32p, abi.f32p], i32),
+        "gd_poses_from_quaternions": ([i32, abi.f32p, abi.f32p], i32),
         "gd_complex_validate": ([C.POINTER(abi.GdComplex)], i32),
         "gd_ctx_create": ([i32, P, C.POINTER(P)], i32),
         "gd_ctx_destroy": ([P], i32),
@@ -141,6 +142,17 @@ def set_temperature(n: int, floor_t: float, ceil_t: float):
     check(load().gd_set_temperature(n, floor_t, ceil_t, abi._ptr(t, C.c_float),
                                     abi._ptr(mb, C.c_float)), "gd_set_temperature")
     return t, mb
+
+
+def poses_from_quaternions(quat_poses: np.ndarray) -> np.ndarray:
+    """[n][7] {tx, ty, tz, qw, qx, qy, qz} -> [n][6] move vectors
+    (gd_poses_from_quaternions)."""
+    q = np.ascontiguousarray(quat_poses, np.float32).reshape(-1, 7)
+    out = np.zeros((q.shape[0], 6), np.float32)
+    check(load().gd_poses_from_quaternions(q.shape[0], abi._ptr(q, C.c_float),
+                                           abi._ptr(out, C.c_float)),
+          "gd_poses_from_quaternions")
+    return out
 
 
 def validate(cx: abi.Complex) -> int:

@@ -127,6 +127,14 @@ gd_status gd_enepara_optimize(const gd_enepara_raw *raw, gd_enepara *out);
 gd_status gd_set_temperature(int n_tmp, float floor_temp, float ceiling_temp,
                              float *temps, float *minus_beta);
 
+/* Rigid poses given as [n_pose][7] {tx, ty, tz, qw, qx, qy, qz} (any
+ * non-zero quaternion; it is normalised) to the [n_pose][6] move vectors
+ * the pose and MC entry points take: the translation, then the ZYX angles
+ * (m3, m4, m5) with R = Rz(m3) Ry(m4) Rx(m5) as Move_d builds it
+ * (move_d.cu:90-105), m4 in [-pi/2, pi/2].  Host only; no context needed.
+ * Zero or non-finite quaternions give GD_EINVAL. */
+gd_status gd_poses_from_quaternions(int n_pose, const float *quat_poses, float *poses);
+
 /* ------------------------------------------------------------------------ */
 /* Inputs (host, caller-owned).  Structure-of-arrays, no capacity caps.      */
 /* ------------------------------------------------------------------------ */
