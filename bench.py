@@ -20,7 +20,8 @@ roofline  the MC-interval kernel: 36 algorithmic FP32 flops per ligand-protein
           pair x pairs per launch / mean launch time (CUDA events), against the
           FP32 FMA peak measured live on this GPU.
 cpu_baseline  the CPU oracle (C port of the reference kernels, OpenMP) on a
-          bounded sample of the same workload on this host.
+          bounded sample of the same workload on this host, on all cores
+          (value) and on one thread (value_1_thread).
 
 --impl reference times the reference's CPU path (the oracle port; the
 reference's own code is CUDA-4/sm_20 only) on all host cores.
@@ -158,11 +159,17 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
     t0 = time.perf_counter()
     done = orc.mc_sample(cx, params, 0, n_rep, n_steps, threads, native)
     dt = time.perf_counter() - t0
+    # one thread as well, on about a fifth of the budget
+    n_steps1 = max(1, min(2000, int(budget_s / 5 / per)))
+    t0 = time.perf_counter()
+    done1 = orc.mc_sample(cx, params, 0, 1, n_steps1, 1, native)
+    dt1 = time.perf_counter() - t0
     return {"value": done / dt, "unit": "replica-MC-steps/s", "cores": threads,
-            "kind": "port",
+            "kind": "port", "value_1_thread": done1 / dt1,
             "sample": f"{n_rep} of {n_rep_total} replicas x {n_steps} MC steps "
                       f"({done} energy evaluations, {dt:.1f} s, "
-                      f"{'-march=native' if native else 'x86-64'} OpenMP build)"}
+                      f"{'-march=native' if native else 'x86-64'} OpenMP build); "
+                      f"1 thread: 1 replica x {n_steps1} MC steps ({dt1:.1f} s)"}
 
 
 def profile_metric(workload, key):
