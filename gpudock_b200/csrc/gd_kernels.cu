@@ -373,62 +373,69 @@ struct PairConst {
   float2 one, lj1, lj0, ca, cb;
 };
 
-// Terms of one atom pair (h) of this lane against one protein point (Ap),
-// two atoms per packed instruction: soft LJ, far-field electrostatics
-// (per-atom sums of ele/d), contact PMF and, with HDB, the H-bond term.  The
-// LJ and PMF quotients share one reciprocal: with D1 = p4 and
-// D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the point
-// type's entry of atom pair 0 of this warp's pair tables.
-__device__ __forceinline__ void pair_hh(const bool hdb, float2 nx, float2 ny, float2 nz,
-                                        const float4 &Ap, const float4 *pp, const float4 *hp,
-                                        int h,
-                                        const PairConst &K, float2 &fvdw, float2 &fpmf,
-                                        float2 &fhdb, float2 &fek, float &mn) {
-  const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
-  const float4 T1 = pp[h * 2 * PT_ROWS + 1];  // -pmf0, pmf1
-  const float2 dx = add2(dup2(Ap.x), nx);
-  const float2 dy = add2(dup2(Ap.y), ny);
-  const float2 dz = add2(dup2(Ap.z), nz);
-  const float2 d2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-  const float2 r = make_float2(frsqrt(d2.x), frsqrt(d2.y));
-  const float2 d = mul2(d2, r);
-  const float2 r2 = mul2(r, r);
-  const float2 r3 = mul2(r2, r);
-  const float2 r6 = mul2(r3, r3);
-  const float2 t9 = mul2(lo2(T0), r3);  // p1a r^3, beside r^6
-  const float2 p1 = mul2(t9, r6);
-  const float2 p12 = fma2(hi2(T0), r6, p1);  // p1 - p2
-  const float2 p4 = fma2(p1, fma2(K.lj1, d2, K.lj0), K.one);
-  const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
-  const float2 ex = make_float2(fex2(arg.x), fex2(arg.y));
-  // D1 D2 and num1 D2 as single FMAs: p4 (1 + ex) = p4 ex + p4
-  const float2 den = fma2(p4, ex, p4);
-  const float2 inv = make_float2(frcp(den.x), frcp(den.y));
-  fvdw = fma2(fma2(p12, ex, p12), inv, fvdw);
-  fpmf = fma2(mul2(hi2(T1), p4), inv, fpmf);
-  fek = fma2(dup2(Ap.w), r, fek);
-  mn = fminf(mn, fminf(d2.x, d2.y));
-  if (hdb) {  // a compile-time constant at every (inlined, unrolled) call
-    // weight 0 (and h3 = 0) for the atoms of the pair without the term
-    const float4 H = hp[h * PT_ROWS];  // -hdb0, w
-    const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
-    const float2 ha = mul2(mul2(h3, h3), K.ca);  // -0.5 log2(e) h3^2
-    fhdb = fma2(hi2(H), make_float2(fex2(ha.x), fex2(ha.y)), fhdb);
-  }
-}
-
-// One protein point against this lane's NA atoms (branch-free body).  The
-// H-bond term runs for the first NHB atom pairs only: H-bond-capable atoms
-// come first in the slot order, so the later pairs of a warp have none.
+// One protein point (A0) against this lane's NA atoms, two atoms per packed
+// instruction (atom pair h): soft LJ, far-field electrostatics (per-atom
+// sums of ele/d), contact PMF and, for the first NHB atom pairs, the H-bond
+// term (H-bond-capable atoms come first in the slot order, so the later
+// pairs of a warp have none; weight 0 and hdb0 = 0 for an atom of a pair
+// without it).  The LJ and PMF quotients share one reciprocal: with D1 = p4
+// and D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the
+// point type's entry of atom pair 0 of this warp's pair tables.
+// Branch-free and written in stages over all atom pairs -- distances and
+// rsqrt, then powers, PMF argument and exp, then the shared reciprocals and
+// sums, then the H-bond Gaussians -- so that the MUFU operations of one
+// stage overlap the FMA work of the others; each accumulator still adds its
+// atom pairs in order h = 0, 1, ...
 template <int NH, int NHB>
 __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                             const float2 (&nz)[NH], const float4 &A0,
                                             const float4 *pp, const float4 *hp,
                                             const PairConst &K, float2 &fvdw, float2 &fpmf,
                                             float2 &fhdb, float2 (&fek)[NH], float &mn) {
+  float2 d2[NH], r[NH];
 #pragma unroll
-  for (int h = 0; h < NH; ++h)  // unrolled: h < NHB folds to a constant
-    pair_hh(h < NHB, nx[h], ny[h], nz[h], A0, pp, hp, h, K, fvdw, fpmf, fhdb, fek[h], mn);
+  for (int h = 0; h < NH; ++h) {
+    const float2 dx = add2(dup2(A0.x), nx[h]);
+    const float2 dy = add2(dup2(A0.y), ny[h]);
+    const float2 dz = add2(dup2(A0.z), nz[h]);
+    d2[h] = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    r[h] = make_float2(frsqrt(d2[h].x), frsqrt(d2[h].y));
+  }
+  float2 ex[NH], p4[NH], p12[NH], pm[NH];
+#pragma unroll
+  for (int h = 0; h < NH; ++h) {
+    const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
+    const float4 T1 = pp[h * 2 * PT_ROWS + 1];  // -pmf0, pmf1
+    const float2 d = mul2(d2[h], r[h]);
+    const float2 r2 = mul2(r[h], r[h]);
+    const float2 r3 = mul2(r2, r[h]);
+    const float2 r6 = mul2(r3, r3);
+    const float2 t9 = mul2(lo2(T0), r3);  // p1a r^3, beside r^6
+    const float2 p1 = mul2(t9, r6);
+    p12[h] = fma2(hi2(T0), r6, p1);  // p1 - p2
+    p4[h] = fma2(p1, fma2(K.lj1, d2[h], K.lj0), K.one);
+    pm[h] = mul2(hi2(T1), p4[h]);
+    const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
+    ex[h] = make_float2(fex2(arg.x), fex2(arg.y));
+  }
+#pragma unroll
+  for (int h = 0; h < NH; ++h) {
+    // D1 D2 and num1 D2 as single FMAs: p4 (1 + ex) = p4 ex + p4
+    const float2 den = fma2(p4[h], ex[h], p4[h]);
+    const float2 inv = make_float2(frcp(den.x), frcp(den.y));
+    fvdw = fma2(fma2(p12[h], ex[h], p12[h]), inv, fvdw);
+    fpmf = fma2(pm[h], inv, fpmf);
+    fek[h] = fma2(dup2(A0.w), r[h], fek[h]);
+    mn = fminf(mn, fminf(d2[h].x, d2[h].y));
+  }
+#pragma unroll
+  for (int h = 0; h < (NHB < NH ? NHB : NH); ++h) {
+    const float2 d = mul2(d2[h], r[h]);
+    const float4 H = hp[h * PT_ROWS];  // -hdb0, w
+    const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
+    const float2 ha = mul2(mul2(h3, h3), K.ca);  // -0.5 log2(e) h3^2
+    fhdb = fma2(hi2(H), make_float2(fex2(ha.x), fex2(ha.y)), fhdb);
+  }
 }
 
 // The fast path over points j0 .. j1-1 of a staged tile, one point per
@@ -444,15 +451,21 @@ __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const flo
                                                const PairConst &K, float thr_l, float2 &fvdw,
                                                float2 &fpmf, float2 &fhdb, float2 (&fek)[NH]) {
   uint32_t close = 0u;
+  // the next point's record is read one iteration ahead
+  float4 Ap = ta[j0];
+  int pt = (int)(__float_as_uint(tb[j0].y) & META_TYPE_MASK);
 #pragma unroll 2
   for (int j = j0; j < j1; ++j) {
-    const float4 Ap = ta[j];
-    const int pt = (int)(__float_as_uint(tb[j].y) & META_TYPE_MASK);
+    const int jn = min(j + 1, j1 - 1);
+    const float4 An = ta[jn];
+    const int ptn = (int)(__float_as_uint(tb[jn].y) & META_TYPE_MASK);
     float mn = 3.0e38f;
     pair_block1<NH, NHB>(nx, ny, nz, Ap, my_ptab + pt * 2, my_htab + pt, K, fvdw, fpmf, fhdb,
                          fek, mn);
     const float thr = __shfl_sync(0xffffffffu, thr_l, j - j0);
     close |= (__any_sync(0xffffffffu, mn <= thr) ? 1u : 0u) << (j - j0);
+    Ap = An;
+    pt = ptn;
   }
   return close;
 }
