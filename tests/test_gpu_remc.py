@@ -215,12 +215,14 @@ def test_gd_run_matches_handles(ctx):
 
 
 def test_remc_distributions_match_oracle(ctx):
-    """Per-temperature energy distributions and acceptance rates of the GPU
-    run against the CPU oracle run, on independent samples: 64 exchange
-    groups of identical starting conformations evolve independently, so the
-    final state of each group is one independent draw of the same law for
-    both implementations; the GPU and CPU runs use different random streams.
-    Two-sample KS per temperature, Welch t on per-group acceptance counts."""
+    """Per-temperature energy distributions, acceptance rates and exchange
+    rates of the GPU run against the CPU oracle run, on independent samples:
+    64 exchange groups of identical starting conformations evolve
+    independently, so the final state of each group is one independent draw
+    of the same law for both implementations; the GPU and CPU runs use
+    different random streams.  Two-sample KS per temperature, Welch t on
+    per-group acceptance counts, Fisher's exact test on accepted / rejected
+    swap attempts; every p-value must exceed 0.01."""
     spec = synth.ComplexSpec(pnp=500, lna=12, n_prt=1, n_lig=1)
     cx = synth.make_complex(spec, seed=26)
     cx.lig_xyz = np.repeat(cx.lig_xyz[:1], 64, axis=0)  # 64 independent groups
@@ -231,6 +233,7 @@ def test_remc_distributions_match_oracle(ctx):
     scale = (0.2, 0.2, 0.2, 0.3, 0.3, 0.3)
     flags = abi.MC_EXCHANGE | abi.MC_MOVE_AWAY
     gpu_e, cpu_e, gpu_a, cpu_a = [], [], [], []
+    swaps = {"gpu": 0, "cpu": 0}
     for k in range(4):
         r = lib.Remc(d, steps, spe, mb, scale, seed=2000 + k, flags=flags)
         r.init()
@@ -240,11 +243,23 @@ def test_remc_distributions_match_oracle(ctx):
         for out, es, acs in ((g, gpu_e, gpu_a), (c, cpu_e, cpu_a)):
             es.append((out.energy[:, abi.E_TOTAL], out.idx_tmp.copy()))
             acs.append(out.acs_mc.reshape(n_tmp, 64).sum(axis=0))
+        # a swap credits both replica slots of the pair
+        swaps["gpu"] += g.ac_temp_exchg // 2
+        swaps["cpu"] += c.ac_temp_exchg // 2
     for t in range(n_tmp):
         a = np.concatenate([e[it == t] for e, it in gpu_e])
         b = np.concatenate([e[it == t] for e, it in cpu_e])
         assert len(a) == len(b) == 4 * 64
         p = stats.ks_2samp(a, b).pvalue
-        assert p > 1e-3, (t, p)
+        assert p > 0.01, (t, p)
     p = stats.ttest_ind(np.concatenate(gpu_a), np.concatenate(cpu_a), equal_var=False).pvalue
-    assert p > 1e-3, p
+    assert p > 0.01, p
+    # attempts: after every interval, in each of the 64 groups, the pairs
+    # (2j + mode, 2j + mode + 1) with mode alternating 0, 1 by round
+    rounds = steps // spe
+    per_mode = [n_tmp // 2, n_tmp // 2 - (n_tmp % 2 == 0)]
+    attempts = 4 * 64 * sum(per_mode[k % 2] for k in range(rounds))
+    assert 0 < swaps["gpu"] < attempts and 0 < swaps["cpu"] < attempts
+    table = [[swaps["gpu"], attempts - swaps["gpu"]], [swaps["cpu"], attempts - swaps["cpu"]]]
+    p = stats.fisher_exact(table).pvalue
+    assert p > 0.01, (table, p)
