@@ -549,6 +549,14 @@ def main():
             except Exception as exc:  # reported, not fatal
                 cpu = {"value": None, "error": str(exc)}
         peaks = measured_peaks()
+        traffic = profile_traffic(w.name)
+        hbm_peak = peaks.get("hbm_gbs")
+        hbm = {"achieved_gbs": traffic / mean_launch_s / 1e9 if traffic else None,
+               "peak_gbs": hbm_peak,
+               "frac": traffic / mean_launch_s / 1e9 / hbm_peak if traffic and hbm_peak
+               else None,
+               "note": "DRAM bytes per launch (ncu) / mean launch time, against the measured "
+                       "copy bandwidth of MEASURED_PEAKS.json: the kernel is not HBM-bound"}
         line = {
             "metric": "replica-MC-steps/s", "value": value, "unit": "replica-MC-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -562,7 +570,7 @@ def main():
                        "parallelism": f"replicas, {ws} independent ensemble(s)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": profile_traffic(w.name),
+                         "traffic": traffic, "hbm": hbm,
                          "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per "
                                            "launch, ncu capture summarised in profiles/",
                          "ncu_pipe_util_pct": {
