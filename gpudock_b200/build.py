@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libgpudock.so")
 SOURCES = ["gd_kernels.cu", "gd_api.cu", "gd_ensemble.cu", "gd_server.cu", "gd_noalloc.cu",
-           "gd_load.cpp"]
+           "gd_similarity.cu", "gd_load.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -34,6 +34,7 @@ def _declare(lib):
         "gd_enepara_optimize": ([C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara)], i32),
         "gd_set_temperature": ([i32, C.c_float, C.c_float, abi.f32p, abi.f32p], i32),
         "gd_poses_from_quaternions": ([i32, abi.f32p, abi.f32p], i32),
+        "gd_similarity_matrix": ([P, P, i32, abi.f32p, abi.f32p], i32),
         "gd_complex_validate": ([C.POINTER(abi.GdComplex)], i32),
         "gd_ctx_create": ([i32, P, C.POINTER(P)], i32),
         "gd_ctx_destroy": ([P], i32),
@@ -256,6 +257,19 @@ class DeviceComplex:
             self.ctx.h, self.h, prt_conf, lig_conf, n, abi._ptr(poses, C.c_float),
             abi._ptr(terms, C.c_float), abi._ptr(rw, C.c_double)), "gd_energy_poses")
         return terms, rw
+
+    def similarity_matrix(self, confs: np.ndarray) -> np.ndarray:
+        """Contact-mode similarity matrix [n, n] of conformations [n, 8]
+        (trace-file rows: protein conf, ligand conf, move vector)
+        (gd_similarity_matrix)."""
+        confs = np.ascontiguousarray(confs, np.float32).reshape(-1, 8)
+        n = confs.shape[0]
+        out = np.zeros((n, n), np.float32)
+        check(self.ctx._lib.gd_similarity_matrix(self.ctx.h, self.h, n,
+                                                  abi._ptr(confs, C.c_float),
+                                                  abi._ptr(out, C.c_float)),
+              "gd_similarity_matrix")
+        return out
 
     def energy_poses_dev(self, n: int, poses_ptr: int, terms_ptr: int, raw_ptr: int = 0,
                          prt_conf: int = 0, lig_conf: int = 0):
@@ -576,6 +590,47 @@ def read_trajectory(directory: str, stem: str):
 
 
 LOAD_PEPTIDE_ALL_MODELS = 0x1
+
+
+def read_traces(path: str) -> np.ndarray:
+    """A trace file of the similarity-matrix tool as read2D reads it
+    (SimilarityMatirxGen util.C:211-240): lines that start with a digit, one
+    conformation each (protein conf, ligand conf, move vector), numbers read
+    as floats until the first that does not parse."""
+    libc = C.CDLL(None)
+    libc.strtof.restype = C.c_float
+    libc.strtof.argtypes = [C.c_char_p, C.POINTER(C.c_char_p)]
+    rows = []
+    with open(path) as f:
+        for line in f:
+            if not line[:1].isdigit():
+                continue
+            row = []
+            for tok in line.split():
+                buf = C.create_string_buffer(tok.encode())
+                end = C.c_char_p()
+                v = libc.strtof(buf, C.byref(end))
+                used = C.cast(end, C.c_void_p).value - C.addressof(buf)
+                if used == 0:
+                    break
+                row.append(v)
+                if used < len(tok):  # a number followed by other characters
+                    break
+            rows.append(row)
+    if not rows:
+        return np.zeros((0, 8), np.float32)
+    return np.asarray(rows, np.float32)
+
+
+def save_similarity(path: str, S: np.ndarray) -> None:
+    """The similarity-matrix file as SaveSimilarityMatrix writes it
+    (SimilarityMatirxGen util.C:128-144): the size, then one row per line,
+    values in the stream's default format (6 significant digits)."""
+    S = np.asarray(S, np.float32)
+    with open(path, "w") as f:
+        f.write(f"{S.shape[0]}\n")
+        for row in S:
+            f.write(" ".join(f"{float(v):g}" for v in row) + "\n")
 
 
 def load_enepara(ff: str, weights: str | None = None, nor_a: str | None = None,

@@ -396,6 +396,20 @@ gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *dcx,
                                   const float *poses, float *terms,
                                   double *raw);
 
+/* Contact-mode similarity matrix of trajectory conformations
+ * (SimilarityMatirxGen CalculateSimilarityMatrix, util.C:37-193).
+ * confs[n_conf][8] are the rows of a trace file: protein conformation and
+ * ligand conformation (as floats, truncated to int), then the move vector
+ * (6).  similarity[n_conf][n_conf] (host) gets, at (i, j), the Matthews
+ * correlation of conformation j's contacts (ligand atom / protein point with
+ * dst <= pmf0) against conformation i's contact map, or GD_CMCC_INVALID
+ * where it is undefined, computed with the reference's float arithmetic:
+ * identical to the reference's values.  Conformations out of the complex's
+ * range, or non-finite values, give GD_EINVAL.  Device memory: about
+ * n_conf * (4 n_conf + lna * pnp / 8) bytes, freed before returning. */
+gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *dcx, int n_conf,
+                               const float *confs, float *similarity);
+
 /* ------------------------------------------------------------------------ */
 /* Replica-exchange Monte Carlo                                             */
 /* ------------------------------------------------------------------------ */

@@ -553,6 +553,72 @@ float orc_mcc(const gd_complex *cx, int ref_prt, int prt_conf, int lig_conf,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Contact-mode similarity matrix (SimilarityMatirxGen src/util.C:37-87     */
+/* CalculateSimilarityMatrix, :90-110 InitConfMatrix, :146-193              */
+/* CalculateContactModeScore).  confs[n][8] = trace rows {protein conf,     */
+/* ligand conf, move[6]}; S[i][j] = the MCC of conformation j's contacts    */
+/* against conformation i's map.  Each conformation's map is built once     */
+/* (PlaceLigand + the dst <= pmf0 test) and kept as bits; the four counts   */
+/* of a pair are those of the reference's double loop, and the score uses   */
+/* its arithmetic: float products of the sums, sqrtf, the integer numerator */
+/* tp tn - fp fn (two's-complement wrap, as the reference's int on the      */
+/* machines it ran on).                                                     */
+/* ------------------------------------------------------------------------ */
+static float orc_contact_mcc(int tp, int fn, int fpc, int tn)
+{
+  const float dividend =
+      sqrtf((float)(tp + fpc) * (float)(tp + fn) * (float)(tn + fpc) * (float)(tn + fn));
+  const int num = (int)((unsigned)tp * (unsigned)tn - (unsigned)fpc * (unsigned)fn);
+  return dividend != 0.0f ? (float)num / dividend : GD_CMCC_INVALID;
+}
+
+void orc_similarity_matrix(const gd_complex *cx, int n, const float *confs, float *S)
+{
+  const int lna = cx->lig.lna;
+  const size_t npair = (size_t)lna * cx->prt.pnp;
+  const size_t nw = (npair + 63) / 64;
+  uint64_t *maps = (uint64_t *)calloc(nw * (size_t)(n > 0 ? n : 1), sizeof(uint64_t));
+  int *pop = (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int i = 0; i < n; ++i) {
+    const float *t = confs + (size_t)8 * i;
+    float *buf = (float *)malloc(sizeof(float) * 3 * (size_t)lna);
+    unsigned char *c = (unsigned char *)malloc(npair);
+    float center[3];
+    orc_place(cx, (int)t[1], t + 2, buf, buf + lna, buf + 2 * lna, center);
+    orc_contacts(cx, (int)t[0], buf, buf + lna, buf + 2 * lna, c);
+    uint64_t *w = maps + nw * (size_t)i;
+    int cnt = 0;
+    for (size_t k = 0; k < npair; ++k)
+      if (c[k]) {
+        w[k >> 6] |= (uint64_t)1 << (k & 63);
+        ++cnt;
+      }
+    pop[i] = cnt;
+    free(c);
+    free(buf);
+  }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int i = 0; i < n; ++i) {
+    const uint64_t *a = maps + nw * (size_t)i;
+    for (int j = 0; j < n; ++j) {
+      const uint64_t *b = maps + nw * (size_t)j;
+      int tp = 0;
+      for (size_t k = 0; k < nw; ++k) tp += __builtin_popcountll(a[k] & b[k]);
+      const int fn = pop[i] - tp, fpc = pop[j] - tp;
+      const int tn = (int)npair - tp - fn - fpc;
+      S[(size_t)i * n + j] = orc_contact_mcc(tp, fn, fpc, tn);
+    }
+  }
+  free(pop);
+  free(maps);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Replica-exchange Monte Carlo                                             */
 /* ------------------------------------------------------------------------ */
 typedef struct orc_rep {

@@ -56,6 +56,7 @@ def load(native: bool = False):
     lib.orc_mc_sample.argtypes = [C.POINTER(abi.GdComplex), C.POINTER(abi.GdMcParams), C.c_int,
                                   C.c_int, C.c_int, C.c_int]
     lib.orc_mc_sample.restype = C.c_longlong
+    lib.orc_similarity_matrix.argtypes = [C.POINTER(abi.GdComplex), C.c_int, P, P]
     lib.orc_max_threads.restype = C.c_int
     lib.orc_mcc.argtypes = [C.POINTER(abi.GdComplex), C.c_int, C.c_int, C.c_int, P]
     lib.orc_mcc.restype = C.c_float
@@ -157,6 +158,15 @@ def mcc(cx: abi.Complex, ref_prt: int, prt_conf: int, lig_conf: int, m) -> float
     mv = np.ascontiguousarray(m, np.float32).reshape(6)
     return float(load().orc_mcc(C.byref(cx.struct()), ref_prt, prt_conf, lig_conf,
                                 mv.ctypes.data))
+
+
+def similarity_matrix(cx: abi.Complex, confs: np.ndarray) -> np.ndarray:
+    """Contact-mode similarity matrix [n, n] of trace rows [n, 8]."""
+    confs = np.ascontiguousarray(confs, np.float32).reshape(-1, 8)
+    n = confs.shape[0]
+    out = np.zeros((n, n), np.float32)
+    load().orc_similarity_matrix(C.byref(cx.struct()), n, _p(confs), _p(out))
+    return out
 
 
 def bayes_total(e) -> np.ndarray:
