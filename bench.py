@@ -378,6 +378,30 @@ def form_poses(ctx, stream, seed, n_pose=1 << 20):
     return {"workload": w.name, "n_pose": n_pose, "by_protein_points": out}
 
 
+def form_similarity(ctx, cx, seed, n_conf=4096):
+    """Contact-mode similarity matrix of n_conf conformations of the headline
+    complex (random protein / ligand conformations, moves of ~1.5 A and
+    ~0.3 rad about the pocket), through gd_similarity_matrix with host
+    buffers: matrix entries per second of the whole call."""
+    from gpudock_b200 import lib
+    rng = np.random.Generator(np.random.PCG64(seed + 5))
+    confs = np.zeros((n_conf, 8), np.float32)
+    confs[:, 0] = rng.integers(0, cx.n_prt, n_conf)
+    confs[:, 1] = rng.integers(0, cx.n_lig, n_conf)
+    confs[:, 2:5] = rng.normal(0.0, 1.5, (n_conf, 3))
+    confs[:, 5:8] = rng.normal(0.0, 0.3, (n_conf, 3))
+    d = lib.DeviceComplex(ctx, cx)
+    d.similarity_matrix(confs[:64])  # warm-up
+    t0 = time.perf_counter()
+    S = d.similarity_matrix(confs)
+    dt = time.perf_counter() - t0
+    d.close()
+    return {"workload": f"similarity_{n_conf}", "n_conf": n_conf,
+            "value": n_conf * n_conf / dt, "unit": "contact-MCC entries/s", "ms": dt * 1e3,
+            "median_entry": float(np.median(S)),
+            "path": "gd_similarity_matrix: host conformations in, host matrix out"}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU path (oracle port) on all cores."""
     ws, rank, _ = dist_env()
@@ -532,6 +556,7 @@ def main():
         for name, fn in (("plain", lambda: form_plain(ctx, stream, args.seed, flush)),
                          ("batched", lambda: form_batched(ctx, stream, args.seed, flush)),
                          ("poses", lambda: form_poses(ctx, stream, args.seed)),
+                         ("similarity", lambda: form_similarity(ctx, cx, args.seed)),
                          ("served", lambda: form_served(args.seed)),
                          # the top of the trace's rate range: the requests arrive
                          # faster than they finish, so this measures capacity
