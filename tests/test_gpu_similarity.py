@@ -74,3 +74,33 @@ def test_argument_checks(ctx):
     # the context still works afterwards
     assert np.array_equal(d.similarity_matrix(confs[:3]), orc.similarity_matrix(cx, confs[:3]))
     d.close()
+
+
+def test_ragged_sizes_and_shared_protein(ctx):
+    """A 120-atom ligand against 1,000 points (the last word of every atom
+    row is part padding), and a complex that uses another's protein
+    conformation 1 as its own conformation 0."""
+    raw, _, _ = synth.default_ff()
+    rng = np.random.Generator(np.random.PCG64(34))
+    prt = synth.make_protein(rng, synth.ComplexSpec(pnp=1000, lna=8, n_prt=2), 8.0, raw)
+    a = synth.make_complex(synth.ComplexSpec(pnp=1000, lna=120, n_prt=2, n_lig=2), seed=35,
+                           protein=prt)
+    b = synth.make_complex(synth.ComplexSpec(pnp=1000, lna=33, n_prt=2, n_lig=3), seed=36,
+                           protein=prt)
+    n = 150
+    confs = np.zeros((n, 8), np.float32)
+    confs[:, 1] = rng.integers(0, 2, n)
+    confs[:, 2:5] = rng.normal(0.0, 1.0, (n, 3))
+    confs[:, 5:8] = rng.normal(0.0, 0.2, (n, 3))
+    da = lib.DeviceComplex(ctx, a)
+    confs[:, 0] = rng.integers(0, 2, n)
+    assert np.array_equal(da.similarity_matrix(confs), orc.similarity_matrix(a, confs))
+    db = lib.DeviceComplex(ctx, b, share=da, prt_conf0=1, n_prt=1)
+    cb = confs.copy()
+    cb[:, 0] = 0
+    cb[:, 1] = rng.integers(0, 3, n)
+    ref = cb.copy()
+    ref[:, 0] = 1  # conformation 0 of the shared view is the protein's conformation 1
+    assert np.array_equal(db.similarity_matrix(cb), orc.similarity_matrix(b, ref))
+    db.close()
+    da.close()
