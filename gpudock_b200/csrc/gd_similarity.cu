@@ -130,6 +130,13 @@ __global__ void __launch_bounds__(kSimThreads)
   __shared__ uint32_t sb[kPairTile][kPairChunk + 1];
   const int i0 = blockIdx.y * kPairTile, j0 = blockIdx.x * kPairTile;
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  // Carry-save counting (Harley and Seal; Mula, Kurz and Lemire, "Faster
+  // population counts using AVX2 instructions", 2018): the AND words of an
+  // entry are added bitwise into `ones` and `twos`; every 4 words the carry
+  // out, `fours`, goes through one POPC (which issues on the XU pipe, 16 per
+  // clock per SM) and the rest stays in bitwise operations.  The count is
+  // 4 sum popc(fours) + 2 popc(twos) + popc(ones).
+  uint32_t ones[4][4] = {}, twos[4][4] = {};
   int acc[4][4] = {};
   for (int k0 = 0; k0 < Kp; k0 += kPairChunk) {
     for (int q = tid; q < kPairTile * kPairChunk; q += kSimThreads) {
@@ -139,20 +146,44 @@ __global__ void __launch_bounds__(kSimThreads)
       sb[row][col] = j < n ? comp[(size_t)j * Kp + k0 + col] : 0u;
     }
     __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < kPairChunk; ++kk) {
-      uint32_t a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = sa[ty + 16 * r][kk];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = sb[tx + 16 * c][kk];
+    for (int kk = 0; kk < kPairChunk; kk += 4) {
+      uint32_t a[4][4], b[4][4];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] += __popc(a[r] & b[c]);
+        for (int q = 0; q < 4; ++q) a[r][q] = sa[ty + 16 * r][kk + q];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) b[c][q] = sb[tx + 16 * c][kk + q];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint32_t x0 = a[r][0] & b[c][0], x1 = a[r][1] & b[c][1];
+          const uint32_t x2 = a[r][2] & b[c][2], x3 = a[r][3] & b[c][3];
+          uint32_t &o = ones[r][c], &t = twos[r][c];
+          // (twos_a, ones) = ones + x0 + x1; (twos_b, ones) = ones + x2 + x3
+          uint32_t u = o ^ x0;
+          const uint32_t ta = (o & x0) | (u & x1);
+          o = u ^ x1;
+          u = o ^ x2;
+          const uint32_t tb = (o & x2) | (u & x3);
+          o = u ^ x3;
+          // (fours, twos) = twos + twos_a + twos_b
+          u = t ^ ta;
+          const uint32_t fours = (t & ta) | (u & tb);
+          t = u ^ tb;
+          acc[r][c] += __popc(fours);
+        }
     }
     __syncthreads();
   }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      acc[r][c] = 4 * acc[r][c] + 2 * __popc(twos[r][c]) + __popc(ones[r][c]);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i = i0 + ty + 16 * r;
