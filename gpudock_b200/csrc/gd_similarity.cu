@@ -221,12 +221,14 @@ struct SimBuffers {
 
 using namespace gd;
 
-extern "C" gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
-                                          const float *confs, float *similarity) {
+// The matrix into S_dev (the caller's device memory) or, with S_dev null,
+// into S_host through a buffer of its own.
+static gd_status similarity_run(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
+                                const float *confs, float *S_dev, float *S_host) {
   if (!ctx || !d) return fail(GD_EINVAL, "gd_similarity_matrix: NULL handle");
   if (n_conf < 0) return fail(GD_EINVAL, "n_conf=%d", n_conf);
   if (n_conf == 0) return GD_OK;
-  if (!confs || !similarity) return fail(GD_EINVAL, "confs/similarity NULL");
+  if (!confs || (!S_dev && !S_host)) return fail(GD_EINVAL, "confs/similarity NULL");
   const KTables &T = d->T;
   if ((size_t)n_conf * (size_t)n_conf > ((size_t)1 << 40))
     return fail(GD_EINVAL, "n_conf=%d: the matrix is too large", n_conf);
@@ -276,7 +278,8 @@ extern "C" gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *d, int
     if (e == cudaSuccess) e = B.get(&d_bits, n * K);
     if (e == cudaSuccess) e = B.get(&d_pop, n);
     if (e == cudaSuccess) e = B.get(&d_mask, K);
-    if (e == cudaSuccess) e = B.get(&d_S, n * n);
+    if (e == cudaSuccess && !S_dev) e = B.get(&d_S, n * n);
+    if (S_dev) d_S = S_dev;
     if (e != cudaSuccess) return fail(GD_ENOMEM, "similarity buffers: %s", cudaGetErrorString(e));
     GD_CUDA(cudaMemcpyAsync(d_conf, hc.data(), sizeof(SimConf) * n, cudaMemcpyHostToDevice, s));
     contacts_kernel<<<n_conf, kSimThreads, sizeof(float4) * T.lna, s>>>(T, d_conf, d_bits, d_pop,
@@ -311,9 +314,22 @@ extern "C" gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *d, int
                                                             d_S);
     GD_CUDA(cudaGetLastError());
     ctx->launches += Kp ? 4 : 3;
-    GD_CUDA(cudaMemcpyAsync(similarity, d_S, sizeof(float) * n * n, cudaMemcpyDeviceToHost, s));
+    if (!S_dev)
+      GD_CUDA(cudaMemcpyAsync(S_host, d_S, sizeof(float) * n * n, cudaMemcpyDeviceToHost, s));
     st = ctx_check(ctx);
   }
   if (st == GD_OK) GD_CUDA(cudaStreamSynchronize(s));
   return st;
+}
+
+extern "C" gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
+                                          const float *confs, float *similarity) {
+  if (n_conf > 0 && !similarity) return fail(GD_EINVAL, "similarity NULL");
+  return similarity_run(ctx, d, n_conf, confs, nullptr, similarity);
+}
+
+extern "C" gd_status gd_similarity_matrix_dev(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
+                                              const float *confs, float *similarity_dev) {
+  if (n_conf > 0 && !similarity_dev) return fail(GD_EINVAL, "similarity_dev NULL");
+  return similarity_run(ctx, d, n_conf, confs, similarity_dev, nullptr);
 }

@@ -35,6 +35,7 @@ def _declare(lib):
         "gd_set_temperature": ([i32, C.c_float, C.c_float, abi.f32p, abi.f32p], i32),
         "gd_poses_from_quaternions": ([i32, abi.f32p, abi.f32p], i32),
         "gd_similarity_matrix": ([P, P, i32, abi.f32p, abi.f32p], i32),
+        "gd_similarity_matrix_dev": ([P, P, i32, abi.f32p, P], i32),
         "gd_complex_validate": ([C.POINTER(abi.GdComplex)], i32),
         "gd_ctx_create": ([i32, P, C.POINTER(P)], i32),
         "gd_ctx_destroy": ([P], i32),
@@ -270,6 +271,15 @@ class DeviceComplex:
                                                   abi._ptr(out, C.c_float)),
               "gd_similarity_matrix")
         return out
+
+    def similarity_matrix_dev(self, confs: np.ndarray, out_ptr: int) -> None:
+        """The matrix into device memory at out_ptr (n * n floats)
+        (gd_similarity_matrix_dev)."""
+        confs = np.ascontiguousarray(confs, np.float32).reshape(-1, 8)
+        check(self.ctx._lib.gd_similarity_matrix_dev(self.ctx.h, self.h, confs.shape[0],
+                                                      abi._ptr(confs, C.c_float),
+                                                      C.c_void_p(out_ptr)),
+              "gd_similarity_matrix_dev")
 
     def energy_poses_dev(self, n: int, poses_ptr: int, terms_ptr: int, raw_ptr: int = 0,
                          prt_conf: int = 0, lig_conf: int = 0):

@@ -17,6 +17,10 @@
  *   SetReplica       gpudocksm-rem-1.2/src/util.C:538-558
  *   loadProtein / loadLigand / loadLHM
  *                    gpudocksm-rem-1.2/src/load.C:100-420, 595-990, 1011-1126
+ *   loadEnePara / loadWeight / loadNorPara
+ *                    gpudocksm-rem-1.2/src/load.C:1139-1419
+ *   CalculateSimilarityMatrix
+ *                    SimilarityMatirxGen/src/util.C:37-193
  */
 #ifndef GPUDOCK_H
 #define GPUDOCK_H
@@ -409,6 +413,11 @@ gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *dcx,
  * n_conf * (4 n_conf + lna * pnp / 8) bytes, freed before returning. */
 gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *dcx, int n_conf,
                                const float *confs, float *similarity);
+/* The same matrix written to device memory of the context's device
+ * (similarity_dev: n_conf * n_conf floats), for callers that keep it on the
+ * GPU; confs stay host memory.  Returns when the matrix is complete. */
+gd_status gd_similarity_matrix_dev(gd_ctx *ctx, const gd_dcomplex *dcx, int n_conf,
+                                   const float *confs, float *similarity_dev);
 
 /* ------------------------------------------------------------------------ */
 /* Replica-exchange Monte Carlo                                             */

@@ -5,6 +5,7 @@ larger synthetic trajectory, including conformations without contacts, a
 single conformation and the argument checks."""
 import numpy as np
 import pytest
+import torch
 
 from gpudock_b200 import abi, lib, synth
 from oracle import oracle as orc
@@ -26,7 +27,12 @@ def test_reference_sample(ctx):
     confs, want = golden()
     d = lib.DeviceComplex(ctx, cx)
     S = d.similarity_matrix(confs)
+    # the device-output entry point writes the same matrix
+    out = torch.full((len(confs), len(confs)), -1.0, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    d.similarity_matrix_dev(confs, out.data_ptr())
     d.close()
+    assert np.array_equal(out.cpu().numpy(), S)
     assert np.array_equal(S, orc.similarity_matrix(cx, confs))
     assert np.all(np.abs(S - want) <= printed_tolerance(want))
 
