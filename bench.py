@@ -390,16 +390,26 @@ def form_similarity(ctx, cx, seed, n_conf=4096):
     confs[:, 1] = rng.integers(0, cx.n_lig, n_conf)
     confs[:, 2:5] = rng.normal(0.0, 1.5, (n_conf, 3))
     confs[:, 5:8] = rng.normal(0.0, 0.3, (n_conf, 3))
+    import torch
     d = lib.DeviceComplex(ctx, cx)
     d.similarity_matrix(confs)  # warm-up: grows the stream-ordered pool to this size
     t0 = time.perf_counter()
     S = d.similarity_matrix(confs)
     dt = time.perf_counter() - t0
+    # the matrix left in device memory (gd_similarity_matrix_dev)
+    out = torch.empty((n_conf, n_conf), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    d.similarity_matrix_dev(confs, out.data_ptr())
+    t0 = time.perf_counter()
+    d.similarity_matrix_dev(confs, out.data_ptr())
+    dt_dev = time.perf_counter() - t0
     d.close()
     return {"workload": f"similarity_{n_conf}", "n_conf": n_conf,
             "value": n_conf * n_conf / dt, "unit": "contact-MCC entries/s", "ms": dt * 1e3,
+            "ms_device_output": dt_dev * 1e3,
             "median_entry": float(np.median(S)),
-            "path": "gd_similarity_matrix: host conformations in, host matrix out"}
+            "path": "gd_similarity_matrix: host conformations in, host matrix out "
+                    "(ms_device_output: gd_similarity_matrix_dev, matrix left on the GPU)"}
 
 
 def run_reference(args):
