@@ -130,12 +130,33 @@ def measured_peaks():
         return {}
 
 
-def build_workload(name, seed):
+def build_workload(name, seed, oracle_tables=False):
+    """(workload, complex, minus_beta).  oracle_tables: derive the kernel
+    tables and the temperature ladder with the oracle's restatements of
+    OptimizeEnepara / SetTemperature (bit-identical to the library's), so
+    that the reference arm never loads the library."""
     from gpudock_b200 import synth
     w = synth.WORKLOADS[name]
-    cx = synth.make_complex(w.spec, seed=seed)
-    _, mb = synth.temperatures(w)
+    if oracle_tables:
+        from oracle import oracle as orc
+        ff = orc.enepara_optimize(synth.raw_ff()[1])
+        cx = synth.make_complex(w.spec, seed=seed, ff=ff)
+        _, mb = synth.temperatures(w, orc.set_temperature)
+    else:
+        cx = synth.make_complex(w.spec, seed=seed)
+        _, mb = synth.temperatures(w)
     return w, cx, mb
+
+
+def workload_config(w, cx, ws):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": w.name, "n_rep": cx.n_prt * cx.n_lig * w.n_tmp, "n_prt": cx.n_prt,
+            "n_lig": cx.n_lig, "n_tmp": w.n_tmp, "lna": cx.lna, "pnp": cx.pnp,
+            "steps_per_exchange": w.steps_per_exchange,
+            "step": f"one exchange interval ({w.steps_per_exchange} MC steps of every replica "
+                    "+ one temperature exchange)",
+            "l2": "GPU arm: flushed (256 MiB write) before every step",
+            "parallelism": f"replicas, {ws} independent ensemble(s)"}
 
 
 def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
@@ -393,21 +414,27 @@ def form_similarity(ctx, cx, seed, n_conf=4096):
     import torch
     d = lib.DeviceComplex(ctx, cx)
     d.similarity_matrix(confs)  # warm-up: grows the stream-ordered pool to this size
-    t0 = time.perf_counter()
-    S = d.similarity_matrix(confs)
-    dt = time.perf_counter() - t0
-    # the matrix left in device memory (gd_similarity_matrix_dev)
-    out = torch.empty((n_conf, n_conf), dtype=torch.float32, device="cuda")
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        S = d.similarity_matrix(confs)
+        times.append(time.perf_counter() - t0)
+    dt = statistics.median(times)
+    # the matrix left in device memory (gd_similarity_matrix_dev), on ctx's device
+    out = torch.empty((n_conf, n_conf), dtype=torch.float32, device=f"cuda:{ctx.device}")
     torch.cuda.synchronize()
     d.similarity_matrix_dev(confs, out.data_ptr())
-    t0 = time.perf_counter()
-    d.similarity_matrix_dev(confs, out.data_ptr())
-    dt_dev = time.perf_counter() - t0
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        d.similarity_matrix_dev(confs, out.data_ptr())
+        times.append(time.perf_counter() - t0)
+    dt_dev = statistics.median(times)
     d.close()
     return {"workload": f"similarity_{n_conf}", "n_conf": n_conf,
             "value": n_conf * n_conf / dt, "unit": "contact-MCC entries/s", "ms": dt * 1e3,
             "ms_device_output": dt_dev * 1e3,
-            "median_entry": float(np.median(S)),
+            "median_entry": float(np.median(S)), "timing": "median of 3 calls each",
             "path": "gd_similarity_matrix: host conformations in, host matrix out "
                     "(ms_device_output: gd_similarity_matrix_dev, matrix left on the GPU)"}
 
@@ -417,7 +444,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    w, cx, mb = build_workload(args.workload, args.seed)
+    w, cx, mb = build_workload(args.workload, args.seed, oracle_tables=True)
     from gpudock_b200 import abi
     from oracle import oracle as orc
     native = True
@@ -447,8 +474,7 @@ def run_reference(args):
         "unit": "replica-MC-steps/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": w.name, "n_rep": n_rep_total, "lna": cx.lna, "pnp": cx.pnp,
-                   "steps_per_exchange": w.steps_per_exchange},
+        "config": workload_config(w, cx, ws),
         "cpu_baseline": {"value": val, "unit": "replica-MC-steps/s", "cores": threads,
                          "kind": "port",
                          "sample": f"per step {n_rep} replicas x 2 MC steps (C oracle, OpenMP)"},
@@ -597,12 +623,7 @@ def main():
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name, "n_rep": n_rep, "n_prt": cx.n_prt,
-                       "n_lig": cx.n_lig, "n_tmp": w.n_tmp, "lna": cx.lna, "pnp": cx.pnp,
-                       "steps_per_exchange": spe, "step": "one exchange interval",
-                       "tile_A_P_NA": list(tile),
-                       "l2": "flushed (256 MiB write) before every step",
-                       "parallelism": f"replicas, {ws} independent ensemble(s)"},
+            "config": workload_config(w, cx, ws),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic, "hbm": hbm,
@@ -619,6 +640,7 @@ def main():
                                      "kernel from the committed ncu capture; frac counts the 36 "
                                      "algorithmic flops per pair against the FFMA peak"},
                          "kernel": "dock_kernel<REMC> (MC interval)",
+                         "tile_A_P_NA": list(tile),
                          "flops_per_launch": FLOP_PER_PAIR * pairs_per_launch,
                          "mean_launch_ms": mean_launch_s * 1e3, "launches": mc_n,
                          "peak_source": "measured live: FP32 FMA probe kernel on this GPU",

@@ -401,6 +401,15 @@ extern "C" gd_status gd_ctx_create(int device, void *stream, gd_ctx **out) {
     delete c;
     return fail(GD_ENOMEM, "cudaMalloc error word: %s", cudaGetErrorString(e));
   }
+  // the fixed scratch of gd_energy_poses_noalloc is committed now, not on
+  // that entry point's first call
+  const gd_status st = noalloc_attach(c);
+  if (st != GD_OK) {
+    cudaFree(c->d_err);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return st;
+  }
   *out = c;
   return GD_OK;
 }

@@ -75,6 +75,9 @@ struct gd_ctx {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_done;
   cudaEvent_t forked = nullptr;
+  // address of the library's fixed pose-scratch array in the CUDA context
+  // that was current when this gd_ctx was created (gd_energy_poses_noalloc)
+  unsigned char *noalloc_scratch = nullptr;
 };
 
 struct gd_dcomplex {
@@ -97,6 +100,10 @@ void dcx_release(gd_dcomplex *d);
 gd_status ctx_check(gd_ctx *c);
 // Status for a nonzero kernel error word (KRun.err).
 gd_status kernel_error(int code);
+// Loads the module that holds the fixed pose-scratch array of
+// gd_energy_poses_noalloc on c's device (current) and stores the array's
+// address in c->noalloc_scratch (gd_noalloc.cu).  Called by gd_ctx_create.
+gd_status noalloc_attach(gd_ctx *c);
 // Ligand-size bucket: sizes are rounded up to a multiple of 8 atoms; launch
 // shapes are chosen (and autotuned) per bucket and cover its largest size.
 int lna_bucket(int lna);

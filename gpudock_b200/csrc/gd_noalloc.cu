@@ -13,7 +13,6 @@
 // call before the launch, and the kernel writes every terms/raw element of the
 // n_pose poses it is given, so nothing in it has to start at zero.
 #include <cstring>
-#include <mutex>
 
 #include "gd_common.h"
 
@@ -34,30 +33,24 @@ static_assert(kScratchBytes < (3u << 20), "pose scratch is meant to stay a few M
 // One copy per device (each device's context has its own instance).
 static __device__ __align__(256) unsigned char g_pose_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
 
-// Resolves the scratch array's address on `device`, which must be current.
-// The lookup is made once per device, on the first call there.
-gd_status scratch_for(int device, unsigned char **out) {
-  if (device < 0 || device >= kMaxDevices)
-    return gd::fail(GD_EINVAL, "gd_energy_poses_noalloc: device %d outside [0, %d)", device,
-                    kMaxDevices);
-  std::lock_guard<std::mutex> g(g_mu);
-  if (!g_scratch_ptr[device]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_pose_scratch);
-    if (e != cudaSuccess || !p)
-      return gd::fail(GD_ECUDA, "gd_energy_poses_noalloc: cudaGetSymbolAddress: %s",
-                      cudaGetErrorString(e));
-    g_scratch_ptr[device] = static_cast<unsigned char *>(p);
-  }
-  *out = g_scratch_ptr[device];
+// Module loading is lazy (CUDA 12): the module that holds g_pose_scratch is
+// loaded, and the array committed on the device, the first time anything of
+// it is touched.  Touching it here, when the context is created, means that
+// a later gd_energy_poses_noalloc call neither loads a module nor commits
+// memory.  The address belongs to the CUDA context current now; a gd_ctx
+// does not outlive that context (after cudaDeviceReset, create a new gd_ctx).
+gd_status gd::noalloc_attach(gd_ctx *c) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_pose_scratch);
+  if (e != cudaSuccess || !p)
+    return gd::fail(e == cudaErrorMemoryAllocation ? GD_ENOMEM : GD_ECUDA,
+                    "gd_ctx_create: address of the pose scratch array: %s",
+                    cudaGetErrorString(e));
+  c->noalloc_scratch = static_cast<unsigned char *>(p);
   return GD_OK;
 }
-
-}  // namespace
 
 extern "C" gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *d, int prt_conf,
                                              int lig_conf, int n_pose, const float *poses,
@@ -69,15 +62,16 @@ extern "C" gd_status gd_energy_poses_noalloc(gd_ctx *ctx, const gd_dcomplex *d, 
                     "gd_energy_poses_noalloc: n_pose=%d exceeds the %d poses its fixed "
                     "scratch holds; split the call or use gd_energy_poses",
                     n_pose, GD_NOALLOC_MAX_POSES);
+  // an empty call succeeds whatever the indices, as gd_energy_poses does
+  if (n_pose == 0) return GD_OK;
   if (prt_conf < 0 || prt_conf >= d->T.n_prt)
     return gd::fail(GD_EINVAL, "prt_conf %d outside [0, %d)", prt_conf, d->T.n_prt);
   if (lig_conf < 0 || lig_conf >= d->T.n_lig)
     return gd::fail(GD_EINVAL, "lig_conf %d outside [0, %d)", lig_conf, d->T.n_lig);
-  if (n_pose == 0) return GD_OK;
   if (!poses || !terms) return gd::fail(GD_EINVAL, "poses/terms NULL");
+  unsigned char *base = ctx->noalloc_scratch;
+  if (!base) return gd::fail(GD_EINVAL, "gd_energy_poses_noalloc: context has no scratch address");
   GD_CUDA(cudaSetDevice(ctx->device));
-  unsigned char *base = nullptr;
-  GD_TRY(scratch_for(ctx->device, &base));
   KItem *d_item = reinterpret_cast<KItem *>(base);
   float *d_poses = reinterpret_cast<float *>(base + kItemBytes);
   float *d_terms = reinterpret_cast<float *>(base + kItemBytes + kPoseBytes);

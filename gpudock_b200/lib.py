@@ -173,6 +173,7 @@ class Context:
         check(self._lib.gd_ctx_create(device, C.c_void_p(stream) if stream else None,
                                       C.byref(h)), "gd_ctx_create")
         self.h = h
+        self.device = device
 
     def sync(self):
         check(self._lib.gd_ctx_sync(self.h), "gd_ctx_sync")

@@ -92,12 +92,20 @@ WORKLOADS = {
 _FF_CACHE = {}
 
 
+def raw_ff():
+    """(raw dict, GdEneparaRaw) of the packaged force field (no library call)."""
+    if "raw" not in _FF_CACHE:
+        raw = forcefield.load_raw()
+        _FF_CACHE["raw"] = (raw, forcefield.raw_struct(raw))
+    return _FF_CACHE["raw"]
+
+
 def default_ff():
-    """(raw dict, GdEneparaRaw, optimised GdEnepara) of the packaged force field."""
+    """(raw dict, GdEneparaRaw, optimised GdEnepara) of the packaged force field,
+    the kernel tables derived by the library's gd_enepara_optimize."""
     if "ff" not in _FF_CACHE:
         from . import lib
-        raw = forcefield.load_raw()
-        rs = forcefield.raw_struct(raw)
+        raw, rs = raw_ff()
         _FF_CACHE["ff"] = (raw, rs, lib.enepara_optimize(rs))
     return _FF_CACHE["ff"]
 
@@ -285,9 +293,15 @@ def make_template(rng, lig_xyz0, lig_t, prt, spec: ComplexSpec, pocket):
     return kde_xyz, kde_t, psp, mcs, tcc
 
 
-def make_complex(spec: ComplexSpec, seed: int, protein: dict | None = None) -> abi.Complex:
-    """A seeded synthetic complex; `protein` reuses an already generated one."""
-    raw, _, ff = default_ff()
+def make_complex(spec: ComplexSpec, seed: int, protein: dict | None = None,
+                 ff: abi.GdEnepara | None = None) -> abi.Complex:
+    """A seeded synthetic complex; `protein` reuses an already generated one.
+    `ff`: kernel tables to attach (default: the packaged force field through
+    the library's gd_enepara_optimize); the generated geometry does not
+    depend on it."""
+    raw, _ = raw_ff()
+    if ff is None:
+        ff = default_ff()[2]
     rng = np.random.Generator(np.random.PCG64(seed))
     lig0, parent = ligand_tree(rng, spec.lna)
     r_lig = float(np.max(np.linalg.norm(lig0, axis=1)))
@@ -330,6 +344,10 @@ def random_poses(rng, n, box=8.0):
     return np.concatenate([t, np.stack([a, b, c], axis=1)], axis=1).astype(np.float32)
 
 
-def temperatures(w: Workload):
-    from . import lib
-    return lib.set_temperature(w.n_tmp, w.t_floor, w.t_ceil)
+def temperatures(w: Workload, set_temperature=None):
+    """(temperatures, minus_beta) of the workload's geometric ladder, from
+    `set_temperature(n, floor, ceiling)` (default: the library's)."""
+    if set_temperature is None:
+        from . import lib
+        set_temperature = lib.set_temperature
+    return set_temperature(w.n_tmp, w.t_floor, w.t_ceil)

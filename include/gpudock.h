@@ -384,10 +384,16 @@ gd_status gd_energy_poses(gd_ctx *ctx, const gd_dcomplex *dcx, int prt_conf,
  * device array compiled into the library (about 2.2 MB per device) instead.
  *
  * Limit: n_pose <= GD_NOALLOC_MAX_POSES; larger calls return GD_EINVAL
- * before anything runs (split them, or use gd_energy_poses).
- * Set-up: the first call on a device looks up the array's address on that
- * device (it must be current; the call makes ctx's device current), so make
- * that first call before any stream capture.
+ * before anything runs (split them, or use gd_energy_poses).  An empty call
+ * (n_pose == 0) returns GD_OK whatever the other arguments, as
+ * gd_energy_poses does.
+ * Set-up: the array is committed on the device, and its address in the
+ * current CUDA context looked up, by gd_ctx_create (CUDA loads the module
+ * that holds it lazily; doing it there keeps the allocation out of this
+ * entry point).  So the calls themselves allocate nothing, and the memory
+ * the array needs is taken when the context is created.  A gd_ctx must not
+ * outlive the CUDA context it was created in: after cudaDeviceReset, create
+ * a new gd_ctx.
  * Nothing in the array has to start at zero: each call writes what the kernel
  * reads before the launch.
  * Overlapping calls race: there is one array per device, shared by every

@@ -1,9 +1,11 @@
 """gd_energy_poses_noalloc: pose energies staged in the library's fixed device
-array instead of allocated buffers. Called through the C-ABI and compared bit
-for bit with gd_energy_poses on two calls in a row (different sizes and
-conformations, so the second call cannot lean on what the first left in the
-shared array). The file sorts last so that it also runs after every other
-GPU test in the same process."""
+array instead of allocated buffers, for callers whose device memory belongs
+to another allocator and that therefore cannot allocate on their scoring path.
+Called through the C-ABI and compared bit for bit with gd_energy_poses on two
+calls in a row (different sizes and conformations, so the second call cannot
+lean on what the first left in the shared array), and checked to leave the
+device's free memory and its stream-ordered pool untouched. The file sorts
+last so that it also runs after every other GPU test in the same process."""
 import ctypes as C
 
 import numpy as np
@@ -57,6 +59,50 @@ def test_noalloc_matches_allocating_entry_point():
     ctx.close()
 
 
+def _memory_state():
+    """(free device bytes, default pool's used and reserved bytes) of device 0."""
+    from cuda.bindings import runtime as rt
+    err, free, _total = rt.cudaMemGetInfo()
+    assert err == rt.cudaError_t.cudaSuccess
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    assert err == rt.cudaError_t.cudaSuccess
+    vals = []
+    for attr in (rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent,
+                 rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent,
+                 rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh):
+        err, v = rt.cudaMemPoolGetAttribute(pool, attr)
+        assert err == rt.cudaError_t.cudaSuccess
+        vals.append(int(v))
+    return int(free), vals, pool
+
+
+def test_noalloc_allocates_nothing():
+    from cuda.bindings import runtime as rt
+    fn = _noalloc_fn()
+    ctx = lib.Context(0)
+    cx = synth.make_complex(synth.ComplexSpec(pnp=900, lna=20), seed=79)
+    d = lib.DeviceComplex(ctx, cx)
+    poses = synth.random_poses(np.random.default_rng(7), 4000, box=3.0)
+    t_ref, r_ref = d.energy_poses(poses)  # the allocating path, first
+    _noalloc(fn, ctx, d, poses, 0, 0)
+    assert rt.cudaDeviceSynchronize()[0] == rt.cudaError_t.cudaSuccess
+    free0, (used0, res0, _), pool = _memory_state()
+    # the pool's high-water mark from here on shows any allocation, even one
+    # freed again before the call returns
+    err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
+                                      rt.cuuint64_t(0))
+    assert err == rt.cudaError_t.cudaSuccess
+    t_na, r_na = _noalloc(fn, ctx, d, poses, 0, 0)
+    assert rt.cudaDeviceSynchronize()[0] == rt.cudaError_t.cudaSuccess
+    free1, (used1, res1, high1), _ = _memory_state()
+    assert np.array_equal(t_na, t_ref) and np.array_equal(r_na, r_ref)
+    assert free1 == free0
+    assert (used1, res1) == (used0, res0)
+    assert high1 <= used0
+    d.close()
+    ctx.close()
+
+
 def test_noalloc_limits():
     fn = _noalloc_fn()
     ctx = lib.Context(0)
@@ -74,8 +120,9 @@ def test_noalloc_limits():
             abi._ptr(terms, C.c_float), None)
     assert st == abi.GD_EINVAL
     assert "exceeds" in lib.last_error()
-    # empty call and bad conformation index
+    # an empty call succeeds whatever the indices, as gd_energy_poses does
     assert fn(ctx.h, d.h, 0, 0, 0, None, None, None) == abi.GD_OK
+    assert fn(ctx.h, d.h, 5, 7, 0, None, None, None) == abi.GD_OK
     st = fn(ctx.h, d.h, 1, 0, 4, abi._ptr(big, C.c_float), abi._ptr(terms, C.c_float), None)
     assert st == abi.GD_EINVAL
     d.close()
