@@ -1,9 +1,10 @@
 """Converts the reference force-field files into data/gpudocksm_ff.npz.
 
-Run in a checkout where the reference project is available; the default
-paths point at its gpudocksm-rem-1.2/test directory:
+Run where the reference project is available, giving its
+gpudocksm-rem-1.2/test directory as the argument (or the reference checkout
+in GD_REFERENCE):
 
-    python -m gpudock_b200.data.make_ff [REFERENCE_TEST_DIR]
+    python -m gpudock_b200.data.make_ff REFERENCE_TEST_DIR
 
 Inputs: gpudocksm.ff (VDW/PMF/HDB/ELE/HPP/HPL/PLJ/PEL/KDE), 08ff_opt (term
 weights), 08_nor_a and 08_nor_b (normalisation a, b), the files the
@@ -16,11 +17,15 @@ import numpy as np
 
 from gpudock_b200 import forcefield
 
-DEFAULT_DIR = "/root/reference/gpudocksm-rem-1.2/test"
 
 
 def main(argv):
-    src = argv[1] if len(argv) > 1 else DEFAULT_DIR
+    if len(argv) > 1:
+        src = argv[1]
+    elif os.environ.get("GD_REFERENCE"):
+        src = os.path.join(os.environ["GD_REFERENCE"], "gpudocksm-rem-1.2", "test")
+    else:
+        sys.exit("usage: python -m gpudock_b200.data.make_ff REFERENCE_TEST_DIR")
 
     def read(name):
         with open(os.path.join(src, name)) as f:

@@ -20,6 +20,20 @@ LIB_NATIVE = os.path.join(HERE, "_build", "libgdoracle_native.so")
 _libs = {}
 
 
+def reference_root():
+    """The reference checkout the checker reads sample inputs and sources
+    from (GD_REFERENCE, else the default of oracle/Makefile.ref), or None
+    where it is absent."""
+    ref = os.environ.get("GD_REFERENCE")
+    if not ref:
+        try:
+            ref = subprocess.run(["make", "-s", "-f", "Makefile.ref", "print-ref"], cwd=HERE,
+                                 capture_output=True, text=True, check=True).stdout.strip()
+        except Exception:
+            return None
+    return ref if ref and os.path.isdir(ref) else None
+
+
 def build(native: bool = False) -> str:
     target = "native" if native else "all"
     path = LIB_NATIVE if native else LIB

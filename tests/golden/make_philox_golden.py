@@ -36,7 +36,9 @@ int main() {
 
 
 def main(argv):
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.environ.get("GD_REFERENCE")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the argument or in GD_REFERENCE")
     inc = os.path.join(ref, "docking", "ising", "src")
     rng = np.random.default_rng(20240601)
     rows = [[0, 0, 0, 0, 0, 0], [0xFFFFFFFF] * 6,

@@ -87,7 +87,9 @@ def golden_lines(ref):
 
 
 def main(argv):
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.environ.get("GD_REFERENCE")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the argument or in GD_REFERENCE")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "-f", "Makefile.ref",
                     f"REF={ref}"], check=True)
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_dump")

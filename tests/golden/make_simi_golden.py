@@ -25,7 +25,9 @@ from gpudock_b200 import lib  # noqa: E402
 
 
 def main(argv):
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.environ.get("GD_REFERENCE")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the argument or in GD_REFERENCE")
     data = os.path.join(ref, "SimilarityMatirxGen", "data")
     confs = lib.read_traces(os.path.join(data, "1a07C1.tr"))
     matrix = np.loadtxt(os.path.join(data, "correct_simi_matrix.txt"), dtype=np.float64)

@@ -1,26 +1,24 @@
-"""The reference-side binding of INTEGRATION.md compiles against the
+"""The reference-side binding integration/run_b200.cc (Run() of
+gpudocksm-rem-1.2/src/run.h on this library) compiles against the
 reference's own headers and links the reference's driver (dock.C + loaders)
 with libgpudock.so into a drop-in linear_dock.  Needs the reference
 checkout; skipped where it is absent (the GPU box)."""
 import os
-import re
 import subprocess
 
 import pytest
 
 from gpudock_b200 import lib
+from oracle.oracle import reference_root
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("GD_REFERENCE", "/root/reference")
+REF = reference_root() or ""
 SRC = os.path.join(REF, "gpudocksm-rem-1.2", "src")
 
 
 @pytest.mark.skipif(not os.path.isdir(SRC), reason="reference sources not available")
 def test_run_shim_links_reference_driver(tmp_path):
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    code = re.findall(r"```cpp\n(.*?)```", text, re.S)[0]
-    shim = tmp_path / "run_b200.cc"
-    shim.write_text(code)
+    shim = os.path.join(ROOT, "integration", "run_b200.cc")
     lib.load()
     libdir = os.path.join(ROOT, "gpudock_b200", "_lib")
     exe = tmp_path / "linear_dock_b200"

@@ -14,9 +14,10 @@ import numpy as np
 import pytest
 
 from gpudock_b200 import abi, forcefield, lib
+from oracle.oracle import reference_root
 from tests.golden_fixture import load_complex
 
-REF = os.environ.get("GD_REFERENCE", "/root/reference")
+REF = reference_root() or ""
 FIELDS = ("lig_xyz", "lig_t", "lig_c", "lig_n", "lig_center", "prt_xyz", "prt_t", "prt_c",
           "prt_ele", "prt_seq3r", "prt_hpcflag", "prt_hpp", "pocket_center", "kde_xyz",
           "kde_t", "mcs_xyz", "mcs_tcc")
