@@ -853,6 +853,16 @@ extern "C" gd_status gd_ctx_set_split(gd_ctx *ctx, int split) {
   return GD_OK;
 }
 
+extern "C" gd_status gd_ctx_set_wait_test(gd_ctx *c, unsigned wait_limit, int never_release) {
+  if (!c) return fail(GD_EINVAL, "ctx is NULL");
+  if (never_release && wait_limit == 0)
+    return fail(GD_EINVAL, "gd_ctx_set_wait_test: never_release needs a wait limit");
+  c->wait_limit = wait_limit;
+  // no run reaches this many MC steps, so a wait for it can only run out
+  c->wait_bias = never_release ? (1 << 30) : 0;
+  return GD_OK;
+}
+
 extern "C" gd_status gd_schedule_pieces(const double *cost, const int *steps, int n_units,
                                         int machines, int *pieces, int cap, int *piece_off,
                                         int *n_used) {

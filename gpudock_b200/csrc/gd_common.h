@@ -67,6 +67,8 @@ struct gd_ctx {
   int sched_mode = 0;      // GD_SCHED_*
   int sched_machines = 0;  // persistent CTAs (0: SMs x occupancy)
   int split_mode = 0;      // CTAs per unit of MC launches (0: split_for's rule)
+  uint32_t wait_limit = 0; // polls of a dependency wait before it gives up (0: default)
+  int wait_bias = 0;       // added to every dependency wait's target (test hook)
   std::atomic<int> refs{1};
   // autotuned launch shapes keyed by (ligand-size bucket, protein tiles)
   std::mutex tile_mu;

@@ -339,6 +339,8 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   R.fused_exchange = pl.fused;
   R.spe = E.spe;
   R.err = E.ctx->d_err;
+  R.wait_limit = E.ctx->wait_limit;
+  R.wait_bias = E.ctx->wait_bias;
   R.hb_pairs = pl.hb_pairs;
   R.split = pl.split;
   return R;
@@ -719,6 +721,116 @@ gd_status ens_read(Ens &E, int i, gd_mc_log *log) {
   return GD_OK;
 }
 
+// Snapshot of a run's state (gd_remc_snapshot / gd_batch_snapshot): a header
+// that identifies the run's shape, then the replica state and counters as
+// the kernels keep them.  The random stream needs no state: Philox is keyed
+// by (seed, stream id) and counted by (replica, step), so restoring the
+// state and the step counter continues the run bit for bit.
+struct SnapHeader {
+  char magic[8];
+  int32_t version, n_items, n_rep_total, step, spe, pad;
+};
+constexpr char kSnapMagic[8] = {'G', 'D', 'S', 'N', 'A', 'P', '1', 0};
+struct SnapItem {
+  int32_t n_rep, n_tmp, lna, pnp;
+  uint64_t seed;
+  uint32_t stream_id, flags;
+};
+
+size_t snap_bytes(const Ens &E) {
+  const size_t n = (size_t)E.n_rep_total;
+  return sizeof(SnapHeader) + sizeof(SnapItem) * E.items.size() +
+         n * sizeof(float) * (6 + GD_NTERM + 1) + n * sizeof(int) * 2 +
+         E.items.size() * MAX_TMP * sizeof(int);
+}
+
+// The state arrays in blob order: {device pointer, bytes}.
+std::vector<std::pair<void *, size_t>> snap_arrays(const Ens &E) {
+  const size_t n = (size_t)E.n_rep_total;
+  return {{E.m_old, n * 6 * sizeof(float)},
+          {E.e_old, n * GD_NTERM * sizeof(float)},
+          {E.cmcc, n * sizeof(float)},
+          {E.idx_tmp, n * sizeof(int)},
+          {E.acs_mc, n * sizeof(int)},
+          {E.acs_exchg, E.items.size() * MAX_TMP * sizeof(int)}};
+}
+
+SnapItem snap_item(const Ens &E, size_t i) {
+  const KItem &I = E.items[i];
+  return SnapItem{I.n_rep, I.n_tmp, I.T.lna, I.T.pnp, E.mc[i].seed, E.mc[i].stream_id,
+                  E.mc[i].flags};
+}
+
+gd_status ens_snapshot(Ens &E, void *buf, size_t cap, size_t *size) {
+  const size_t need = snap_bytes(E);
+  if (size) *size = need;
+  if (!buf) return GD_OK;  // size query
+  if (cap < need) return fail(GD_EINVAL, "snapshot needs %zu bytes, buffer holds %zu", need, cap);
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  GD_TRY(ctx_check(E.ctx));  // the state is complete and no kernel reported an error
+  unsigned char *p = static_cast<unsigned char *>(buf);
+  SnapHeader h{};
+  std::memcpy(h.magic, kSnapMagic, sizeof h.magic);
+  h.version = 1;
+  h.n_items = (int32_t)E.items.size();
+  h.n_rep_total = E.n_rep_total;
+  h.step = E.step;
+  h.spe = E.spe;
+  std::memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  for (size_t i = 0; i < E.items.size(); ++i) {
+    const SnapItem it = snap_item(E, i);
+    std::memcpy(p, &it, sizeof it);
+    p += sizeof it;
+  }
+  for (const auto &a : snap_arrays(E)) {
+    GD_CUDA(cudaMemcpyAsync(p, a.first, a.second, cudaMemcpyDeviceToHost, E.ctx->stream));
+    p += a.second;
+  }
+  GD_CUDA(cudaStreamSynchronize(E.ctx->stream));
+  return GD_OK;
+}
+
+gd_status ens_restore(Ens &E, const void *buf, size_t size) {
+  if (!buf) return fail(GD_EINVAL, "snapshot buffer NULL");
+  if (size != snap_bytes(E))
+    return fail(GD_EINVAL, "snapshot of %zu bytes does not fit this run (%zu bytes)", size,
+                snap_bytes(E));
+  const unsigned char *p = static_cast<const unsigned char *>(buf);
+  SnapHeader h;
+  std::memcpy(&h, p, sizeof h);
+  p += sizeof h;
+  if (std::memcmp(h.magic, kSnapMagic, sizeof h.magic) != 0 || h.version != 1)
+    return fail(GD_EINVAL, "not a run snapshot of this library");
+  if (h.n_items != (int32_t)E.items.size() || h.n_rep_total != E.n_rep_total ||
+      h.spe != E.spe || h.step < 0 || h.step % E.spe != 0)
+    return fail(GD_EINVAL, "snapshot of a run of another shape (items %d, replicas %d, "
+                           "steps per exchange %d, step %d)",
+                h.n_items, h.n_rep_total, h.spe, h.step);
+  for (size_t i = 0; i < E.items.size(); ++i) {
+    SnapItem it;
+    std::memcpy(&it, p, sizeof it);
+    p += sizeof it;
+    const SnapItem mine = snap_item(E, i);
+    if (std::memcmp(&it, &mine, sizeof it) != 0)
+      return fail(GD_EINVAL, "snapshot item %zu has another complex size or random stream", i);
+  }
+  GD_CUDA(cudaSetDevice(E.ctx->device));
+  cudaStream_t s = E.ctx->stream;
+  for (const auto &a : snap_arrays(E)) {
+    GD_CUDA(cudaMemcpyAsync(a.first, p, a.second, cudaMemcpyHostToDevice, s));
+    p += a.second;
+  }
+  // progress words count absolute steps and only ever grow within a run:
+  // start them again below the restored step
+  for (const Plan &pl : E.plans)
+    GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
+  GD_CUDA(cudaStreamSynchronize(s));  // the host buffer may be reused on return
+  E.step = h.step;
+  if (E.traj) E.traj->seq = E.traj->spd > 0 ? h.step / E.traj->spd : 0;
+  return GD_OK;
+}
+
 gd_status ens_kernel_times(Ens &E, double *mc_ms, int *mc_n, double *ex_ms, int *ex_n) {
   GD_CUDA(cudaSetDevice(E.ctx->device));
   GD_CUDA(cudaStreamSynchronize(E.ctx->stream));
@@ -798,6 +910,16 @@ extern "C" gd_status gd_remc_run(gd_remc *r, int n_steps) {
 extern "C" gd_status gd_remc_read(gd_remc *r, gd_mc_log *log) {
   if (!r || !log) return fail(GD_EINVAL, "gd_remc_read: NULL argument");
   return ens_read(r->e, 0, log);
+}
+
+extern "C" gd_status gd_remc_snapshot(gd_remc *r, void *buf, size_t cap, size_t *size) {
+  if (!r) return fail(GD_EINVAL, "remc is NULL");
+  return ens_snapshot(r->e, buf, cap, size);
+}
+
+extern "C" gd_status gd_remc_restore(gd_remc *r, const void *buf, size_t size) {
+  if (!r) return fail(GD_EINVAL, "remc is NULL");
+  return ens_restore(r->e, buf, size);
 }
 
 extern "C" gd_status gd_remc_set_trajectory(gd_remc *r, const char *dir, const char *stem) {
@@ -891,6 +1013,16 @@ extern "C" gd_status gd_batch_run(gd_batch *b, int n_steps) {
 extern "C" gd_status gd_batch_read(gd_batch *b, int item, gd_mc_log *log) {
   if (!b || !log) return fail(GD_EINVAL, "gd_batch_read: NULL argument");
   return ens_read(b->e, item, log);
+}
+
+extern "C" gd_status gd_batch_snapshot(gd_batch *b, void *buf, size_t cap, size_t *size) {
+  if (!b) return fail(GD_EINVAL, "batch is NULL");
+  return ens_snapshot(b->e, buf, cap, size);
+}
+
+extern "C" gd_status gd_batch_restore(gd_batch *b, const void *buf, size_t size) {
+  if (!b) return fail(GD_EINVAL, "batch is NULL");
+  return ens_restore(b->e, buf, size);
 }
 
 extern "C" gd_status gd_batch_set_profiling(gd_batch *b, int on) {

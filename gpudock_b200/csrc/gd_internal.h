@@ -148,6 +148,9 @@ struct KRun {
   int *progress;         // [units] MC steps done (absolute step count)
   int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too
                          // low, 4 a piece's predecessor never finished
+  uint32_t wait_limit;   // polls of a piece's dependency wait (0: 2^24, ~4 s)
+  int wait_bias;         // added to the wait's target: 0, or (test hook) a step
+                         // the predecessor never reaches, so the wait runs out
 };
 
 // McNaughton's wrap-around rule, for MC steps that must run in order: units

@@ -729,7 +729,9 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     }
     // the steps before this piece ran on another CTA: wait until it has
     // written their state back (bounded; code 4 if it never does)
-    if (wait_dep) wait_progress(R.progress + unit, step_base, R.err, 4);
+    if (wait_dep)
+      wait_progress(R.progress + unit, step_base + R.wait_bias, R.err, 4,
+                    R.wait_limit ? R.wait_limit : (1u << 24));
     s_ctl->first_it = it;
     s_ctl->sig_unit = unit;
     s_ctl->sig_step = launch_base + s_hi;

@@ -48,6 +48,11 @@ def _declare(lib):
         "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
         "gd_ctx_set_schedule": ([P, i32, i32], i32),
         "gd_ctx_set_split": ([P, i32], i32),
+        "gd_ctx_set_wait_test": ([P, C.c_uint, i32], i32),
+        "gd_remc_snapshot": ([P, P, C.c_size_t, C.POINTER(C.c_size_t)], i32),
+        "gd_remc_restore": ([P, P, C.c_size_t], i32),
+        "gd_batch_snapshot": ([P, P, C.c_size_t, C.POINTER(C.c_size_t)], i32),
+        "gd_batch_restore": ([P, P, C.c_size_t], i32),
         "gd_load": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                      C.POINTER(abi.GdEneparaRaw), C.POINTER(abi.GdEnepara), C.c_uint,
                      C.POINTER(P)], i32),
@@ -189,6 +194,13 @@ class Context:
     def set_schedule(self, mode: int, machines: int = 0):
         """abi.SCHED_AUTO / SCHED_WAVES / SCHED_PERSISTENT (over `machines` CTAs)."""
         check(self._lib.gd_ctx_set_schedule(self.h, mode, machines), "gd_ctx_set_schedule")
+
+    def set_wait_test(self, wait_limit: int, never_release: bool):
+        """Test hook: dependency waits of later MC launches give up after
+        `wait_limit` polls; with never_release every one of them runs out
+        (gd_ctx_set_wait_test).  set_wait_test(0, False) restores the default."""
+        check(self._lib.gd_ctx_set_wait_test(self.h, int(wait_limit), int(never_release)),
+              "gd_ctx_set_wait_test")
 
     def close(self):
         if self.h:
@@ -345,6 +357,20 @@ class Remc:
                                                      C.byref(nb)), "gd_remc_kernel_times")
         return a.value, na.value, b.value, nb.value
 
+    def snapshot(self) -> bytes:
+        """The run's state as bytes (gd_remc_snapshot): replica state, counters, step."""
+        lib = self.dcx.ctx._lib
+        n = C.c_size_t()
+        check(lib.gd_remc_snapshot(self.h, None, 0, C.byref(n)), "gd_remc_snapshot")
+        buf = C.create_string_buffer(n.value)
+        check(lib.gd_remc_snapshot(self.h, buf, n.value, C.byref(n)), "gd_remc_snapshot")
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        """Loads a snapshot of a run of the same shape (gd_remc_restore)."""
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        check(self.dcx.ctx._lib.gd_remc_restore(self.h, buf, len(blob)), "gd_remc_restore")
+
     def read(self) -> abi.McLogBuffers:
         buf = abi.McLogBuffers(self.n_rep, self.n_tmp, self.steps_total, self.record)
         check(self.dcx.ctx._lib.gd_remc_read(self.h, C.byref(buf.log)), "gd_remc_read")
@@ -392,6 +418,20 @@ class Batch:
         buf = abi.McLogBuffers(n_rep, p.n_tmp, p.steps_total, bool(p.flags & abi.MC_RECORD))
         check(self.ctx._lib.gd_batch_read(self.h, i, C.byref(buf.log)), "gd_batch_read")
         return buf
+
+    def snapshot(self) -> bytes:
+        """The run's state as bytes (gd_batch_snapshot): replica state, counters, step."""
+        lib = self.ctx._lib
+        n = C.c_size_t()
+        check(lib.gd_batch_snapshot(self.h, None, 0, C.byref(n)), "gd_batch_snapshot")
+        buf = C.create_string_buffer(n.value)
+        check(lib.gd_batch_snapshot(self.h, buf, n.value, C.byref(n)), "gd_batch_snapshot")
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        """Loads a snapshot of a run of the same shape (gd_batch_restore)."""
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        check(self.ctx._lib.gd_batch_restore(self.h, buf, len(blob)), "gd_batch_restore")
 
     def _n_rep_of(self, i):
         d = self.dcxs[i]

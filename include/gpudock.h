@@ -520,6 +520,24 @@ gd_status gd_remc_destroy(gd_remc *remc);
  * gd_remc_read. */
 gd_status gd_remc_set_trajectory(gd_remc *remc, const char *dir,
                                  const char *stem);
+/* Checkpoint / resume (no counterpart in the reference, which keeps no
+ * random-number state in its dumps, util_d.cu:85-92, and cannot resume).
+ * gd_remc_snapshot writes the run's state into host memory: a header naming
+ * the run's shape (replicas, temperatures, ligand and protein sizes, seed,
+ * stream id, flags) and step counter, then every replica's accepted move
+ * vector, energy, MCC, temperature index and acceptance counter and the
+ * exchange counters per temperature slot.  With buf == NULL it only sets
+ * *size; otherwise cap must be at least *size.  It waits for the run's
+ * enqueued work and fails with that work's error, if any.
+ * gd_remc_restore loads such a snapshot into a run created with the same
+ * complex sizes and MC parameters (GD_EINVAL otherwise) and sets its step
+ * counter; the next gd_remc_run continues from there.  The random stream is
+ * counter-based (key: seed, stream id; counter: replica, step), so a run
+ * snapshotted at step s and restored into a new handle gives the same
+ * trajectory, bit for bit, as one run without the break.  The in-memory
+ * record (GD_MC_RECORD) of steps before s is not part of a snapshot. */
+gd_status gd_remc_snapshot(gd_remc *remc, void *buf, size_t cap, size_t *size);
+gd_status gd_remc_restore(gd_remc *remc, const void *buf, size_t size);
 int gd_remc_n_rep(const gd_remc *remc);
 /* CUDA-event timing of the MC kernels and exchange kernels issued by
  * gd_remc_run / gd_batch_run while profiling is on.  One MC sample spans the
@@ -558,6 +576,9 @@ gd_status gd_batch_read(gd_batch *batch, int item, gd_mc_log *log);
 gd_status gd_batch_destroy(gd_batch *batch);
 int gd_batch_n_rep(const gd_batch *batch);
 int gd_batch_n_launch_shapes(const gd_batch *batch);
+/* Checkpoint / resume of a whole batch, as gd_remc_snapshot / restore. */
+gd_status gd_batch_snapshot(gd_batch *batch, void *buf, size_t cap, size_t *size);
+gd_status gd_batch_restore(gd_batch *batch, const void *buf, size_t size);
 gd_status gd_batch_set_profiling(gd_batch *batch, int on);
 gd_status gd_batch_kernel_times(gd_batch *batch, double *mc_ms, int *mc_launches,
                                 double *exch_ms, int *exch_launches);
@@ -624,6 +645,19 @@ gd_status gd_expf_dev(gd_ctx *ctx, int n, const float *x, float *y);
  * 8 chains x 16 FMAs x iters each; returns the time and the flop count. */
 gd_status gd_fma_peak(gd_ctx *ctx, int n_blocks, int iters, float *ms,
                       double *flops);
+/* Test hook for the failure path of the persistent schedule's bounded
+ * waits (a CTA that continues a unit waits for the CTA that ran the unit's
+ * earlier steps).  MC launches enqueued through ctx after the call give up
+ * such a wait after wait_limit polls of about 256 ns each (0: the default,
+ * 2^24 polls, about 4 s).  With never_release != 0 every such wait targets
+ * a step no run reaches, so each one runs out after wait_limit polls: the
+ * kernel records the error and finishes, and the next call that checks the
+ * context's error word (gd_remc_read, gd_ctx_sync, ...) returns
+ * GD_ETIMEDOUT and clears it.  The results of such a run are undefined.
+ * never_release needs a nonzero wait_limit.  gd_ctx_set_wait_test(ctx, 0, 0)
+ * restores the defaults (runs created meanwhile keep the setting their
+ * captured launches were built with). */
+gd_status gd_ctx_set_wait_test(gd_ctx *ctx, unsigned wait_limit, int never_release);
 /* The persistent schedule (host only, no device): n_units units of cost[u]
  * per MC step and steps[u] steps over `machines` CTAs.  pieces[4 k ..] =
  * {unit, first step, end step, wait} for k < piece_off[*n_used], CTA m's in
