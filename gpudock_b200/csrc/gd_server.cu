@@ -72,6 +72,7 @@ struct Req {
   gd_dcomplex *dcx = nullptr;
   float *d_m_old = nullptr, *d_e_old = nullptr, *d_mb = nullptr, *d_cmcc = nullptr;
   int *d_idx = nullptr, *d_acs = nullptr, *d_acx = nullptr;
+  gd_record *d_rec = nullptr;     // [n_rep][steps_total] with GD_MC_RECORD
   Lane *lane = nullptr;            // its launch shape
   cudaStream_t stream = nullptr;  // the lane's stream
   int step = 0;
@@ -81,6 +82,7 @@ struct Req {
   // results
   std::vector<float> energy, movematrix;
   std::vector<int> acs, idx, acx;
+  std::vector<gd_record> rec;
 };
 
 // A launch shape of the server (tile, staging, group layout, exchange
@@ -141,8 +143,9 @@ struct gd_server {
 
 namespace {
 
-// Device bytes a request holds while active (tables + replica state).
-size_t request_bytes(const gd_complex *cx, int n_rep) {
+// Device bytes a request holds while active (tables + replica state, and
+// its per-step record with GD_MC_RECORD).
+size_t request_bytes(const gd_complex *cx, const gd_mc_params *mc, int n_rep) {
   size_t b = (size_t)TAB_ROWS * GD_NPT * 24;
   b += (size_t)cx->lig.n_conf * cx->lig.lna * 16 + (size_t)cx->lig.lna * 8;
   b += (size_t)GD_NLT * cx->psp.n_col * 4;
@@ -151,6 +154,7 @@ size_t request_bytes(const gd_complex *cx, int n_rep) {
   b += (size_t)n_rep * (6 + GD_NTERM + 3) * 4 + 3 * MAX_TMP * 4;
   // MCC reference map: one bit per (atom, padded point)
   b += (size_t)cx->lig.lna * ((cx->prt.pnp + TILE_PTS - 1) / TILE_PTS) * (TILE_PTS / 8);
+  if (mc->flags & GD_MC_RECORD) b += (size_t)n_rep * mc->steps_total * sizeof(gd_record);
   return b;
 }
 
@@ -168,8 +172,10 @@ void release_device(Req *r) {
   if (r->d_idx) cudaFreeAsync(r->d_idx, s);
   if (r->d_acs) cudaFreeAsync(r->d_acs, s);
   if (r->d_acx) cudaFreeAsync(r->d_acx, s);
+  if (r->d_rec) cudaFreeAsync(r->d_rec, s);
   r->d_m_old = r->d_e_old = r->d_mb = r->d_cmcc = nullptr;
   r->d_idx = r->d_acs = r->d_acx = nullptr;
+  r->d_rec = nullptr;
   if (r->dcx) {
     cudaStreamSynchronize(s);
     dcx_release(r->dcx);
@@ -244,6 +250,12 @@ gd_status admit(gd_server *S, Req *r) {
   GD_CUDA(cudaMallocAsync(&r->d_acs, n * sizeof(int), s));
   GD_CUDA(cudaMallocAsync(&r->d_acx, MAX_TMP * sizeof(int), s));
   GD_CUDA(cudaMemsetAsync(r->d_acx, 0, MAX_TMP * sizeof(int), s));
+  const bool record = (r->mc.flags & GD_MC_RECORD) != 0;
+  if (record) {
+    const size_t nr = n * (size_t)r->mc.steps_total * sizeof(gd_record);
+    GD_CUDA(cudaMallocAsync((void **)&r->d_rec, nr, s));
+    GD_CUDA(cudaMemsetAsync(r->d_rec, 0, nr, s));
+  }
   GD_CUDA(cudaMemcpyAsync(r->d_mb, r->mb.data(), r->mb.size() * sizeof(float),
                           cudaMemcpyHostToDevice, s));
   KItem &I = r->item;
@@ -259,10 +271,12 @@ gd_status admit(gd_server *S, Req *r) {
   for (int k = 0; k < 6; ++k) I.move_scale[k] = r->mc.move_scale[k];
   I.seed = r->mc.seed;
   I.stream_id = r->mc.stream_id;
-  I.flags = r->mc.flags & ~GD_MC_RECORD;
+  I.flags = r->mc.flags;
   I.minus_beta = r->d_mb;
   I.acs_exchg = r->d_acx;
-  I.record = nullptr;
+  I.record = r->d_rec;  // steps 0 .. steps_total-1 (no ring)
+  I.rec_steps = record ? r->mc.steps_total : 0;
+  I.rec_ring = 0;
   I.m_old = r->d_m_old;
   I.e_old = r->d_e_old;
   I.cmcc = r->d_cmcc;
@@ -402,6 +416,11 @@ gd_status copy_out(Req *r) {
   GD_CUDA(cudaMemcpyAsync(r->acs.data(), r->d_acs, n * 4, cudaMemcpyDeviceToHost, s));
   GD_CUDA(cudaMemcpyAsync(r->idx.data(), r->d_idx, n * 4, cudaMemcpyDeviceToHost, s));
   GD_CUDA(cudaMemcpyAsync(r->acx.data(), r->d_acx, r->mc.n_tmp * 4, cudaMemcpyDeviceToHost, s));
+  if (r->d_rec) {
+    r->rec.resize(n * (size_t)r->mc.steps_total);
+    GD_CUDA(cudaMemcpyAsync(r->rec.data(), r->d_rec, r->rec.size() * sizeof(gd_record),
+                            cudaMemcpyDeviceToHost, s));
+  }
   GD_CUDA(cudaStreamSynchronize(s));
   return GD_OK;
 }
@@ -620,7 +639,7 @@ gd_status copy_request(gd_server *S, int protein_id, const gd_complex *cx,
   r->mc.minus_beta = r->mb.data();
   r->protein = protein_id;
   r->n_rep = P.prt.n_conf * L.n_conf * mc->n_tmp;
-  r->bytes = request_bytes(&r->cx, r->n_rep);
+  r->bytes = request_bytes(&r->cx, &r->mc, r->n_rep);
   return GD_OK;
 }
 
@@ -743,6 +762,8 @@ static gd_status take_result(gd_server *S, std::unordered_map<uint64_t, std::uni
       if (log->acs_mc) std::memcpy(log->acs_mc, r->acs.data(), n * 4);
       if (log->idx_tmp) std::memcpy(log->idx_tmp, r->idx.data(), n * 4);
       if (log->acs_temp_exchg) std::memcpy(log->acs_temp_exchg, r->acx.data(), r->acx.size() * 4);
+      if (log->record && !r->rec.empty())
+        std::memcpy(log->record, r->rec.data(), r->rec.size() * sizeof(gd_record));
       log->ac_mc = 0;
       for (int v : r->acs) log->ac_mc += v;
       log->ac_temp_exchg = 0;

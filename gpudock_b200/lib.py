@@ -485,7 +485,8 @@ class Server:
         check(self._lib.gd_server_submit(self.h, protein_id, C.byref(cx.struct()),
                                          C.byref(params), C.byref(rid)), "gd_server_submit")
         n_rep = n_prt * cx.n_lig * len(mb)
-        self._pending[rid.value] = abi.McLogBuffers(n_rep, len(mb))
+        record = bool(params.flags & abi.MC_RECORD)
+        self._pending[rid.value] = abi.McLogBuffers(n_rep, len(mb), steps_total, record)
         return rid.value
 
     def poll(self, rid: int):

@@ -614,7 +614,10 @@ gd_status gd_server_create(int device, size_t hbm_budget_bytes, int max_active,
 /* Makes the protein (all conformations) of cx resident; returns its id. */
 gd_status gd_server_add_protein(gd_server *srv, const gd_complex *cx, int *protein_id);
 /* Copies the request (cx->prt is ignored: the resident protein is used).
- * GD_EBUDGET when it can never fit the budget. */
+ * GD_EBUDGET when it can never fit the budget.  With GD_MC_RECORD in
+ * mc->flags the request also keeps its per-step record on the device
+ * (n_rep x steps_total gd_record, counted in its budget), returned through
+ * log->record by gd_server_poll / gd_server_wait. */
 gd_status gd_server_submit(gd_server *srv, int protein_id, const gd_complex *cx,
                            const gd_mc_params *mc, uint64_t *req_id);
 /* GD_EAGAIN while queued or running; GD_OK with the results (t_wall = latency

@@ -2,14 +2,14 @@
 not grow with the workload: the headline ensemble (8,800 replicas, 40 atoms x
 4,000 points, 11 protein x 50 ligand conformations x 16 temperatures), the
 512-ligand batch (16,384 replicas against a 6,000-point protein) and the
-1,048,576-pose sweep against 16,000 points.
+1,048,576-pose sweep against 2,000 / 4,000 / 8,000 / 16,000 points.
 
 Checked at those sizes: every Metropolis decision and every exchange round
 replayed bit-exactly from the device's own records; the energies of a seeded
 sample of recorded states against the oracle; the temperature labels of every
 exchange group a permutation at every step; the acceptance counter equal to
 the records; pose energies bit-identical whatever the order of the poses, and
-a seeded sample of them against the oracle."""
+a seeded 4,096-pose subset at each protein size against the oracle."""
 import dataclasses
 import types
 
@@ -118,11 +118,15 @@ def test_batched_512_full_size(ctx):
     base.close()
 
 
-def test_poses_full_size(ctx):
+@pytest.mark.parametrize("pnp", [2000, 4000, 8000, 16000])
+def test_poses_full_size(ctx, pnp):
+    """The 1,048,576-pose sweep at each protein size: a seeded 4,096-pose
+    subset against the oracle, term by term (raw FP64 sums too), and every
+    pose's energy bit-identical whatever the order of the poses."""
     w = synth.WORKLOADS["poses_48"]
     n_pose = 1 << 20
-    cx = synth.make_complex(dataclasses.replace(w.spec, pnp=16000), seed=2024 + 16000)
-    rng = np.random.default_rng(11)
+    cx = synth.make_complex(dataclasses.replace(w.spec, pnp=pnp), seed=2024 + pnp)
+    rng = np.random.default_rng(11 + pnp)
     poses = synth.random_poses(rng, n_pose, box=w.extra["box"])
     perm = rng.permutation(n_pose)
     d = lib.DeviceComplex(ctx, cx)
@@ -130,15 +134,18 @@ def test_poses_full_size(ctx):
     pp = torch.from_numpy(np.ascontiguousarray(poses[perm])).cuda()
     t1 = torch.empty((n_pose, abi.NTERM), dtype=torch.float32, device="cuda")
     t2 = torch.empty_like(t1)
+    r1 = torch.empty((n_pose, abi.NRAW), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()  # the inputs were copied on torch's stream
-    d.energy_poses_dev(n_pose, pd.data_ptr(), t1.data_ptr())
+    d.energy_poses_dev(n_pose, pd.data_ptr(), t1.data_ptr(), r1.data_ptr())
     d.energy_poses_dev(n_pose, pp.data_ptr(), t2.data_ptr())
     ctx.sync()
-    a, b = t1.cpu().numpy(), t2.cpu().numpy()
+    a, b, raw = t1.cpu().numpy(), t2.cpu().numpy(), r1.cpu().numpy()
     d.close()
     assert np.isfinite(a).all()
     assert np.array_equal(a[perm], b)
-    idx = rng.choice(n_pose, 64, replace=False)
+    idx = rng.choice(n_pose, w.extra["parity_subset"], replace=False)
     terms_r, raw_r, asum = orc.energy_poses(cx, poses[idx])
+    bad, rel = tol.check_raw(raw[idx], raw_r, asum)
+    assert not bad.any(), np.nanmax(rel, axis=0)
     bad, rel = tol.check_terms(a[idx], terms_r, raw_r, asum, cx.ff)
     assert not bad.any(), np.nanmax(rel, axis=0)

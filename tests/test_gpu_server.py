@@ -103,3 +103,42 @@ def test_server_errors_and_cancel():
         tiny.submit(pid, cxs[0], 20, 10, mb, n_prt=1)
     assert e.value.status == abi.GD_EBUDGET
     tiny.close()
+
+
+def test_served_records_replay_on_oracle():
+    """Requests recorded through the server (GD_MC_RECORD) while they share
+    launches: every Metropolis decision and every exchange round replays
+    bit-exactly on the oracle from the request's own record, the state
+    follows the decisions, the temperature labels of every exchange group
+    stay a permutation, and a seeded sample of recorded states has the
+    oracle's energies (per term, 1e-5 relative)."""
+    from tests.test_gpu_fullsize import _groups_are_permutations, _sample_energies
+    from tests.test_gpu_remc import _replay_checks
+
+    cxs = _protein_and_ligands(900, [14, 30, 47, 22, 61], seed=52)
+    _, mb = lib.set_temperature(8, 0.004, 0.04)
+    steps, spe, seed = 60, 10, 13
+    kw = dict(flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY | abi.MC_RECORD)
+    srv = lib.Server(0, hbm_budget_bytes=1 << 30, max_active=3, steps_per_launch=20)
+    pid = srv.add_protein(cxs[0])
+    ids = []
+    for i, cx in enumerate(cxs):
+        ids.append(srv.submit(pid, cx, steps, spe, mb, n_prt=1, seed=seed, stream_id=i, **kw))
+        if i == 2:
+            time.sleep(0.02)  # later requests join launches already running
+    swaps = 0
+    for i, (rid, cx) in enumerate(zip(ids, cxs)):
+        out = srv.wait(rid)
+        rec = out.record
+        assert rec.shape == (cx.n_lig * 8, steps)
+        assert np.array_equal(rec["step"][0], np.arange(steps))
+        swaps += _replay_checks(cx, mb, rec, seed, spe, 8, stream=i)
+        _groups_are_permutations(rec, 1, 8, cx.n_lig)
+        assert out.ac_mc == int(rec["accepted"].sum())
+        # the final state is the state after the last recorded decision
+        last = rec[:, -1]
+        e_fin = np.where(last["accepted"] == 1, last["e_prop_total"], last["e"][:, abi.E_TOTAL])
+        assert np.array_equal(out.energy[:, abi.E_TOTAL], e_fin)
+        _sample_energies(cx, rec, np.random.Generator(np.random.PCG64(i)), n_sample=6)
+    assert swaps > 0
+    srv.close()

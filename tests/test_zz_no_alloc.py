@@ -77,6 +77,7 @@ def _memory_state():
 
 
 def test_noalloc_allocates_nothing():
+    from cuda.bindings import driver
     from cuda.bindings import runtime as rt
     fn = _noalloc_fn()
     ctx = lib.Context(0)
@@ -90,7 +91,7 @@ def test_noalloc_allocates_nothing():
     # the pool's high-water mark from here on shows any allocation, even one
     # freed again before the call returns
     err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
-                                      rt.cuuint64_t(0))
+                                      driver.cuuint64_t(0))
     assert err == rt.cudaError_t.cudaSuccess
     t_na, r_na = _noalloc(fn, ctx, d, poses, 0, 0)
     assert rt.cudaDeviceSynchronize()[0] == rt.cudaError_t.cudaSuccess
