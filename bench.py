@@ -193,6 +193,43 @@ def cpu_baseline(w, cx, mb, budget_s=15.0, native=True):
                       f"1 thread: 1 replica x {n_steps1} MC steps ({dt1:.1f} s)"}
 
 
+def cpu_rate(cxs, mb, move_scale, spe, budget_s=3.0):
+    """The oracle's replica-MC-steps/s on a sample of complexes (each complex's
+    replicas in parallel), on all host cores and on one thread: a bounded
+    sample sized to about budget_s seconds per leg."""
+    from gpudock_b200 import abi
+    from oracle import oracle as orc
+    native = True
+    try:
+        orc.build(native=True)
+    except Exception:
+        native = False
+    threads = orc.max_threads(native)
+    params = [abi.mc_params(1000, spe, mb, move_scale, seed=1) for _ in cxs]
+    out = {}
+    for leg, nt in (("all_cores", threads), ("one_thread", 1)):
+        # calibrate on one step of the first complex's replicas
+        n_rep0 = cxs[0].n_prt * cxs[0].n_lig * len(mb)
+        n_rep0 = min(n_rep0, nt * 4) if nt > 1 else 1
+        t0 = time.perf_counter()
+        orc.mc_sample(cxs[0], params[0][0], 0, n_rep0, 1, nt, native)
+        per = max(time.perf_counter() - t0, 1e-5) / n_rep0 * nt  # s per replica-step per thread
+        done, t_used = 0, 0.0
+        for cx, (pa, _keep) in zip(cxs, params):
+            n_rep = cx.n_prt * cx.n_lig * len(mb)
+            n_rep = min(n_rep, max(nt, 1) * 2) if nt > 1 else 1
+            n_steps = max(1, int(budget_s / len(cxs) / (per * n_rep / nt)))
+            t0 = time.perf_counter()
+            done += orc.mc_sample(cx, pa, 0, n_rep, n_steps, nt, native)
+            t_used += time.perf_counter() - t0
+        out[leg] = done / t_used
+    return {"value": out["all_cores"], "unit": "replica-MC-steps/s", "cores": threads,
+            "kind": "port", "value_1_thread": out["one_thread"],
+            "sample": f"{len(cxs)} complex(es) of the form, a replica sample each, "
+                      f"about {budget_s:g} s per leg (C oracle, OpenMP, "
+                      f"{'-march=native' if native else 'x86-64'})"}
+
+
 def profile_metric(workload, key):
     """(value, unit) of one metric row of the committed ncu summary of the
     headline kernel of this workload, or None."""
@@ -250,7 +287,8 @@ def form_plain(ctx, stream, seed, flush):
     d.close()
     return {"workload": w.name, "n_rep": n_rep, "mc_steps": steps,
             "value": n_rep * steps / (ms * 1e-3), "unit": "replica-MC-steps/s",
-            "ms_per_mc_step": ms / steps}
+            "ms_per_mc_step": ms / steps,
+            "cpu_baseline": cpu_rate([cx], mb, w.move_scale, w.steps_per_exchange)}
 
 
 def form_batched(ctx, stream, seed, flush, n_steps=50):
@@ -303,6 +341,9 @@ def form_batched(ctx, stream, seed, flush, n_steps=50):
     cad, table = lib.autotune_cadence(ctx, dcxs[:148], mb, candidates=(1, 2, 5, 10, 20),
                                       steps=40, move_scale=w.move_scale, seed=seed,
                                       flags=abi.MC_EXCHANGE)
+    pick = np.random.Generator(np.random.PCG64(seed + 9)).choice(len(cxs), 8, replace=False)
+    out["cpu_baseline"] = cpu_rate([cxs[i] for i in pick], mb, w.move_scale, w.steps_per_exchange)
+    out["cpu_baseline"]["sample"] = "8 of the 512 ligands; " + out["cpu_baseline"]["sample"]
     out["cadence"] = {"chosen_steps_per_exchange": cad,
                       "ms_per_mc_step": {str(k): v for k, v in table.items()},
                       "sample": "148 of the 512 ligands, 40 MC steps per candidate"}
@@ -312,12 +353,15 @@ def form_batched(ctx, stream, seed, flush, n_steps=50):
     return out
 
 
-def form_served(seed, rate=50.0, n_request=300, steps=2000, budget_gb=120):
+def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool=512,
+                cpu=True, steps_per_launch=None, split=None, max_active=0):
     """Serving form: Poisson arrivals at `rate` req/s; ligand sizes log-normal
     (median 30, clipped to 8..120); each request 4 ligand conformations x 8
     temperatures (32 replicas) x `steps` MC steps against one of 4 resident
     proteins (2,000 / 4,000 / 7,000 / 10,000 points); admission by an HBM
-    budget.  Latency = submit -> result, measured by the server."""
+    budget.  The requests cycle through a pool of `pool` distinct synthetic
+    complexes, each submission with its own random stream.  Latency = submit
+    -> result, measured by the server; the queue is sampled every 0.5 s."""
     import dataclasses
     from gpudock_b200 import abi, lib, synth
     w = synth.WORKLOADS["serving"]
@@ -326,52 +370,106 @@ def form_served(seed, rate=50.0, n_request=300, steps=2000, budget_gb=120):
     prots = [synth.make_protein(rng, dataclasses.replace(w.spec, pnp=p), 10.0, raw)
              for p in w.extra["proteins"]]
     lo, hi = w.extra["lna_clip"]
+    n_pool = min(n_request, pool)
     lnas = np.clip(np.round(np.exp(rng.normal(np.log(w.extra["lna_median"]), 0.5,
-                                              n_request))), lo, hi).astype(int)
-    which = rng.integers(0, len(prots), n_request)
+                                              n_pool))), lo, hi).astype(int)
+    which = rng.integers(0, len(prots), n_pool)
     gaps = rng.exponential(1.0 / rate, n_request)
     cxs = [synth.make_complex(dataclasses.replace(w.spec, lna=int(n),
                                                   pnp=w.extra["proteins"][k]),
                               seed=seed + 1000 + i, protein=prots[k])
            for i, (n, k) in enumerate(zip(lnas, which))]
     _, mb = synth.temperatures(w)
-    srv = lib.Server(0, hbm_budget_bytes=int(budget_gb) << 30, max_active=0,
-                     steps_per_launch=w.steps_per_exchange * 10)
-    pids = []
-    for k in range(len(prots)):
-        first = next(i for i in range(n_request) if which[i] == k) if (which == k).any() else None
-        pids.append(srv.add_protein(cxs[first]) if first is not None else None)
-    ids = []
+    srv = lib.Server(0, hbm_budget_bytes=int(budget_gb) << 30, max_active=max_active,
+                     steps_per_launch=steps_per_launch or w.steps_per_exchange * 10)
+    if split is not None:
+        srv.set_split(split)
+    pids = [srv.add_protein(cxs[int(np.nonzero(which == k)[0][0])]) if (which == k).any()
+            else None for k in range(len(prots))]
+    n_rep = 32
+    pairs = 0.0
+    series = []
+    ids, pending = [], {}
+    lat = np.zeros(n_request)
+    svc = np.zeros(n_request)
+
+    def sample(t0):
+        st = srv.stats()
+        series.append([round(time.perf_counter() - t0, 2), st.queued, st.active,
+                       int(st.completed)])
+
+    def collect():
+        for i in list(pending):
+            out = srv.poll(pending[i])
+            if out is not None:
+                lat[i] = out.log.t_wall
+                svc[i] = out.log.t_compute
+                del pending[i]
+
     t0 = time.perf_counter()
     t_next = t0
-    for i, cx in enumerate(cxs):
+    t_sample = t0
+    for i in range(n_request):
+        k = i % n_pool
         t_next += gaps[i]
-        dt = t_next - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        ids.append(srv.submit(pids[which[i]], cx, steps, w.steps_per_exchange, mb, n_prt=1,
-                              seed=seed, stream_id=i, flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY))
-    lat, svc = [], []
-    for rid in ids:
-        log = srv.wait(rid, timeout_ms=900000).log
-        lat.append(log.t_wall)
-        svc.append(log.t_compute)
+        while True:
+            now = time.perf_counter()
+            if now >= t_sample:
+                sample(t0)
+                collect()
+                t_sample += 0.5
+            if now >= t_next:
+                break
+            time.sleep(min(t_next - now, max(0.0, t_sample - now), 0.01))
+        rid = srv.submit(pids[which[k]], cxs[k], steps, w.steps_per_exchange, mb, n_prt=1,
+                         seed=seed, stream_id=i, flags=abi.MC_EXCHANGE | abi.MC_MOVE_AWAY)
+        ids.append(rid)
+        pending[i] = rid
+        pairs += n_rep * steps * int(lnas[k]) * w.extra["proteins"][which[k]]
+    t_submitted = time.perf_counter() - t0
+    while pending:
+        if time.perf_counter() >= t_sample:
+            sample(t0)
+            t_sample += 0.5
+        collect()
+        time.sleep(0.01)
     wall = time.perf_counter() - t0
+    sample(t0)
     st = srv.stats()
     srv.close()
-    lat = np.asarray(lat)
-    svc = np.asarray(svc)
-    n_rep = 32
-    return {"workload": w.name, "n_request": n_request, "rate_req_s": rate,
-            "mc_steps": steps, "replicas_per_request": n_rep,
-            "value": n_request * n_rep * steps / wall, "unit": "replica-MC-steps/s",
-            "requests_per_s": n_request / wall,
-            "p50_latency_s": float(np.percentile(lat, 50)),
-            "p99_latency_s": float(np.percentile(lat, 99)),
-            "p50_service_s": float(np.percentile(svc, 50)),
-            "p99_service_s": float(np.percentile(svc, 99)),
-            "busy_s": st.busy_s, "launches": st.launches,
-            "sample": f"{n_request} of the 10,000-request trace at {rate:g} req/s"}
+    n_sm = 148
+    try:
+        import torch
+        n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    except Exception:
+        pass
+    skip = n_request // 5  # the first fifth fills the GPU: not steady state
+    out = {"workload": w.name, "n_request": n_request, "rate_req_s": rate,
+           "mc_steps": steps, "replicas_per_request": n_rep,
+           "value": n_request * n_rep * steps / wall, "unit": "replica-MC-steps/s",
+           "requests_per_s": n_request / wall,
+           "fp32_tflops": FLOP_PER_PAIR * pairs / wall / 1e12,
+           "submitted_in_s": t_submitted, "wall_s": wall,
+           "p50_latency_s": float(np.percentile(lat[skip:], 50)),
+           "p99_latency_s": float(np.percentile(lat[skip:], 99)),
+           "p50_latency_all_s": float(np.percentile(lat, 50)),
+           "p99_latency_all_s": float(np.percentile(lat, 99)),
+           "p50_service_s": float(np.percentile(svc[skip:], 50)),
+           "p99_service_s": float(np.percentile(svc[skip:], 99)),
+           "latency_window": f"requests {skip}..{n_request - 1} (after the first fifth)",
+           "sm_occupancy": st.cta_busy_s / (n_sm * wall),
+           "busy_s": st.busy_s, "launches": st.launches,
+           "queue_series": {"every_s": 0.5, "columns": ["t_s", "queued", "active", "completed"],
+                            "rows": series[::4]},
+           "sample": f"{n_request} requests of the 10,000-request trace at {rate:g} req/s, "
+                     f"cycling through {n_pool} distinct synthetic complexes"}
+    if cpu:
+        pick = np.random.Generator(np.random.PCG64(seed + 4)).choice(n_pool, 8, replace=False)
+        out["cpu_baseline"] = cpu_rate([cxs[i] for i in pick], mb, w.move_scale,
+                                       w.steps_per_exchange)
+        out["cpu_baseline"]["sample"] = ("8 of the requests (throughput only); "
+                                         + out["cpu_baseline"]["sample"])
+    return out
 
 
 def form_poses(ctx, stream, seed, n_pose=1 << 20):
@@ -382,7 +480,8 @@ def form_poses(ctx, stream, seed, n_pose=1 << 20):
     from gpudock_b200 import lib, synth
     w = synth.WORKLOADS["poses_48"]
     rng = np.random.default_rng(seed + 3)
-    poses = torch.from_numpy(synth.random_poses(rng, n_pose, box=w.extra["box"])).cuda()
+    poses_h = synth.random_poses(rng, n_pose, box=w.extra["box"])
+    poses = torch.from_numpy(poses_h).cuda()
     terms = torch.empty((n_pose, 10), dtype=torch.float32, device="cuda")
     out = {}
     for pnp in w.extra["pnp_sweep"]:
@@ -394,9 +493,36 @@ def form_poses(ctx, stream, seed, n_pose=1 << 20):
         ms = _event_ms(stream, run)
         out[str(pnp)] = {"value": n_pose / (ms * 1e-3), "unit": "pose-energies/s",
                          "fp32_tflops": FLOP_PER_PAIR * n_pose * cx.lna * pnp / (ms * 1e-3)
-                         / 1e12, "tile": list(tile)}
+                         / 1e12, "tile": list(tile),
+                         "cpu_baseline": cpu_poses_rate(cx, poses_h)}
         d.close()
     return {"workload": w.name, "n_pose": n_pose, "by_protein_points": out}
+
+
+def cpu_poses_rate(cx, poses, budget_s=2.0):
+    """The oracle's pose-energies/s on a prefix of the sweep's poses, on all
+    host cores and on one thread (about budget_s seconds per leg)."""
+    from oracle import oracle as orc
+    native = True
+    try:
+        orc.build(native=True)
+    except Exception:
+        native = False
+    threads = orc.max_threads(native)
+    out = {}
+    for leg, nt in (("all_cores", threads), ("one_thread", 1)):
+        n = nt
+        t0 = time.perf_counter()
+        orc.energy_poses(cx, poses[:n], n_threads=nt, native=native)
+        per = max(time.perf_counter() - t0, 1e-5) / n * nt
+        n = int(min(4096, max(nt, budget_s / per * nt)))
+        t0 = time.perf_counter()
+        orc.energy_poses(cx, poses[:n], n_threads=nt, native=native)
+        out[leg] = (n / (time.perf_counter() - t0), n)
+    return {"value": out["all_cores"][0], "unit": "pose-energies/s", "cores": threads,
+            "kind": "port", "value_1_thread": out["one_thread"][0],
+            "sample": f"{out['all_cores'][1]} poses on all cores, {out['one_thread'][1]} on one "
+                      f"thread (C oracle, {'-march=native' if native else 'x86-64'})"}
 
 
 def form_similarity(ctx, cx, seed, n_conf=4096):
@@ -596,7 +722,8 @@ def main():
                          ("served", lambda: form_served(args.seed)),
                          # the top of the trace's rate range: the requests arrive
                          # faster than they finish, so this measures capacity
-                         ("served_400", lambda: form_served(args.seed, rate=400.0))):
+                         ("served_400", lambda: form_served(args.seed, rate=400.0,
+                                                            cpu=False))):
             try:
                 forms[name] = fn()
             except Exception as exc:  # reported, not fatal

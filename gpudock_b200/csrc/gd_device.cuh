@@ -246,6 +246,13 @@ __device__ __forceinline__ const T *cluster_map(const T *p, int rank) {
   return reinterpret_cast<const T *>(out);
 }
 
+// Nanosecond clock shared by all SMs.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Release store / acquire load of a word at GPU scope (progress flags
 // between CTAs of one launch).
 __device__ __forceinline__ void st_release(int *p, int v) {

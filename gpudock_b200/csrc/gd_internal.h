@@ -34,10 +34,10 @@ constexpr uint32_t META_SEQ_SHIFT = 12u;
 constexpr int MAX_SEQ3R = (1 << 20) - 1;
 // Points past the protein's last point (up to the tile boundary) are padding:
 // type PAD_POINT_TYPE, whose kernel table rows are all zero, no charge, and
-// far from everything (d^9 still finite in FP32 for coordinates within a
-// few thousand A), so the pair loop may run over them and add exactly zero.
+// far from everything (on the opposite side from the padding ligand atoms),
+// so the pair loop may run over them and add exactly zero.
 constexpr int PAD_POINT_TYPE = 31;
-constexpr float PAD_POINT_COORD = -3.0e3f;
+constexpr float PAD_POINT_COORD = -1.0e4f;
 
 enum KMode : int { KMODE_POSES = 0, KMODE_REMC = 1, KMODE_INIT = 2 };
 
@@ -148,6 +148,8 @@ struct KRun {
   int *progress;         // [units] MC steps done (absolute step count)
   int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too
                          // low, 4 a piece's predecessor never finished
+  unsigned long long *busy_ns;  // nullptr, or: each CTA adds the nanoseconds
+                                // from its start to its end (SM occupancy)
   uint32_t wait_limit;   // polls of a piece's dependency wait (0: 2^24, ~4 s)
   int wait_bias;         // added to the wait's target: 0, or (test hook) a step
                          // the predecessor never reaches, so the wait runs out

@@ -41,11 +41,9 @@ namespace gd {
 
 constexpr int STAGE_BYTES = TILE_PTS * (16 + 8);
 constexpr int CHUNK = 32;  // points per FP32 partial before the FP64 flush
-#ifndef GD_POINT_UNROLL
-#define GD_POINT_UNROLL 2
-#endif
-constexpr int kPointUnroll = GD_POINT_UNROLL;  // protein points per iteration of the fast path
+constexpr int kPointUnroll = 2;  // protein points per iteration of the fast path
 constexpr float LOG2E = 1.4426950408889634f;
+constexpr float FAR = 1.0e4f;  // coordinate of the padding atoms
 // Point types of the kernel's pair tables: the force field's GD_NPT plus
 // all-zero rows, one of which (PAD_POINT_TYPE) marks the padding points that
 // fill a tile past the protein's last point, so they add exactly zero.
@@ -376,39 +374,19 @@ struct PairConst {
   float2 one, lj1, lj0, ca, cb;
 };
 
-// Products of two atoms' denominators whose reciprocal is normal and exact
-// enough to share lie in [2^-125, 2^126): their bit pattern minus that of
-// 2^-125 is below kProdSpan as an unsigned integer (zero, infinity and NaN
-// are not).  Outside that range (pairs beyond about 120 A, or closer than
-// 1e-4 A) a lane takes its own two reciprocals instead.
-constexpr uint32_t kProdLow = 0x01000000u;   // 2^-125
-constexpr uint32_t kProdSpan = 0x7E000000u;  // 2^126 - 2^-125 in bits
-__device__ __forceinline__ uint32_t prod_key(float p) { return __float_as_uint(p) - kProdLow; }
-
 // One protein point (A0) against this lane's NA atoms, two atoms per packed
 // instruction (atom pair h): soft LJ, far-field electrostatics (per-atom
 // sums of ele/d), contact PMF and, for the first NHB atom pairs, the H-bond
 // term (H-bond-capable atoms come first in the slot order, so the later
 // pairs of a warp have none; weight 0 and hdb0 = 0 for an atom of a pair
-// without it).  pp / hp point at the point type's entry of atom pair 0 of
-// this warp's pair tables.
-//
-// Soft LJ of calcenergy_d.cu:96-100, (p1 - p2) / p4 with p1 = p1a / d^9,
-// p2 = p2a / d^6, p4 = 1 + p1 L, L = lj0 (1 + lj1 d^2), multiplied through by
-// d^9: (p1a - p2a d^3) / (d^9 + p1a L).  Its denominator D1 stays between
-// p1a L and d^9 (no overflow at short range), and it takes two fewer
-// multiplies than the powers of 1/d.  The LJ and PMF quotients share one
-// reciprocal, with D2 = 1 + exp(.): num1/D1 = num1 D2 / (D1 D2), pmf1/D2 =
-// pmf1 D1 / (D1 D2), and so do the two atoms of a pair: 1/x = y / (x y).  A
-// lane whose product x y falls outside [2^-125, 2^126) takes its own
-// two reciprocals (the branch is warp-uniform and rare; a lane's results
-// never depend on another lane's).
-//
-// Written in stages over all atom pairs -- distances and rsqrt, then
-// powers, PMF argument, exp, denominators and H-bond Gaussians, then the
-// shared reciprocals and sums -- so that the MUFU operations of one stage
-// overlap the FMA work of the others; each accumulator still adds its atom
-// pairs in order h = 0, 1, ...
+// without it).  The LJ and PMF quotients share one reciprocal: with D1 = p4
+// and D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the
+// point type's entry of atom pair 0 of this warp's pair tables.
+// Branch-free and written in stages over all atom pairs -- distances and
+// rsqrt, then powers, PMF argument and exp, then the shared reciprocals and
+// sums, then the H-bond Gaussians -- so that the MUFU operations of one
+// stage overlap the FMA work of the others; each accumulator still adds its
+// atom pairs in order h = 0, 1, ...
 template <int NH, int NHB>
 __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                             const float2 (&nz)[NH], const float4 &A0,
@@ -424,56 +402,48 @@ __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2
     d2[h] = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
     r[h] = make_float2(frsqrt(d2[h].x), frsqrt(d2[h].y));
   }
-  // powers, PMF argument and exp, H-bond Gaussian; D1 D2 and num1 D2 as
-  // single FMAs: D1 (1 + ex) = D1 ex + D1 (d, r and d^2 end here: the
-  // far-field electrostatics and the close-range minimum take them now)
-  float2 den[NH], num[NH], pm[NH];
-  float prod[NH];
-  uint32_t key = 0u;  // largest prod_key of the lane
+  float2 ex[NH], p4[NH], p12[NH], pm[NH];
 #pragma unroll
   for (int h = 0; h < NH; ++h) {
     const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
     const float4 T1 = pp[h * 2 * PT_ROWS + 1];  // -pmf0, pmf1
     const float2 d = mul2(d2[h], r[h]);
+    const float2 r2 = mul2(r[h], r[h]);
+    const float2 r3 = mul2(r2, r[h]);
+    const float2 r6 = mul2(r3, r3);
+    const float2 t9 = mul2(lo2(T0), r3);  // p1a r^3, beside r^6
+    const float2 p1 = mul2(t9, r6);
+    p12[h] = fma2(hi2(T0), r6, p1);  // p1 - p2
+    p4[h] = fma2(p1, fma2(K.lj1, d2[h], K.lj0), K.one);
+    pm[h] = mul2(hi2(T1), p4[h]);
+    const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
+    ex[h] = make_float2(fex2(arg.x), fex2(arg.y));
+  }
+#pragma unroll
+  for (int h = 0; h < NH; ++h) {
+    // D1 D2 and num1 D2 as single FMAs: p4 (1 + ex) = p4 ex + p4
+    const float2 den = fma2(p4[h], ex[h], p4[h]);
+    const float2 inv = make_float2(frcp(den.x), frcp(den.y));
+    fvdw = fma2(fma2(p12[h], ex[h], p12[h]), inv, fvdw);
+    fpmf = fma2(pm[h], inv, fpmf);
     fek[h] = fma2(dup2(A0.w), r[h], fek[h]);
     mn = fminf(mn, fminf(d2[h].x, d2[h].y));
-    const float2 g = mul2(d2[h], d);            // d^3
-    const float2 g3 = mul2(mul2(g, g), g);      // d^9
-    const float2 den1 = fma2(lo2(T0), fma2(K.lj1, d2[h], K.lj0), g3);  // d^9 + p1a L
-    const float2 num1 = fma2(hi2(T0), g, lo2(T0));                      // p1a - p2a d^3
-    pm[h] = mul2(hi2(T1), den1);
-    const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
-    const float2 ex = make_float2(fex2(arg.x), fex2(arg.y));
-    den[h] = fma2(den1, ex, den1);
-    num[h] = fma2(num1, ex, num1);
-    prod[h] = __fmul_rn(den[h].x, den[h].y);
-    key = max(key, prod_key(prod[h]));
-    if (h < NHB) {
-      const float4 H = hp[h * PT_ROWS];  // -hdb0, w
-      const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
-      const float2 ha = mul2(mul2(h3, h3), K.ca);  // -0.5 log2(e) h3^2
-      fhdb = fma2(hi2(H), make_float2(fex2(ha.x), fex2(ha.y)), fhdb);
-    }
   }
-  // the shared reciprocals and the sums
-  if (!__any_sync(0xffffffffu, key >= kProdSpan)) {
 #pragma unroll
-    for (int h = 0; h < NH; ++h) {
-      const float2 inv = mul2(make_float2(den[h].y, den[h].x), dup2(frcp(prod[h])));
-      fvdw = fma2(num[h], inv, fvdw);
-      fpmf = fma2(pm[h], inv, fpmf);
-    }
-  } else {  // rare: lanes with a product out of range take their own reciprocals
-#pragma unroll
-    for (int h = 0; h < NH; ++h) {
-      float2 inv = mul2(make_float2(den[h].y, den[h].x), dup2(frcp(prod[h])));
-      if (prod_key(prod[h]) >= kProdSpan) inv = make_float2(frcp(den[h].x), frcp(den[h].y));
-      fvdw = fma2(num[h], inv, fvdw);
-      fpmf = fma2(pm[h], inv, fpmf);
-    }
+  for (int h = 0; h < (NHB < NH ? NHB : NH); ++h) {
+    const float2 d = mul2(d2[h], r[h]);
+    const float4 H = hp[h * PT_ROWS];  // -hdb0, w
+    const float2 h3 = mul2(add2(d, lo2(H)), hi2(H));
+    const float2 ha = mul2(mul2(h3, h3), K.ca);  // -0.5 log2(e) h3^2
+    fhdb = fma2(hi2(H), make_float2(fex2(ha.x), fex2(ha.y)), fhdb);
   }
 }
 
+// The fast path over points j0 .. j1-1 of a staged tile, one point per
+// iteration and no branch in the body, so the compiler can overlap one
+// point's tail with the next point's head.  Returns the mask of points whose
+// close-range terms must run: some lane has an atom within the point's
+// threshold (thr_l, held by lane j - j0).  NHB: atom pairs with the H-bond term.
 template <int NH, int NHB>
 __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                                const float2 (&nz)[NH], const float4 *ta,
@@ -610,6 +580,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   // With a schedule (PIECES, R.pieces) a CTA's number is a ticket taken when it
   // starts (wrapping back to 0 after the last CTA), so a CTA only ever waits
   // on one that started before it.
+  const unsigned long long t_start = R.busy_ns ? global_ns() : 0ull;
   if (threadIdx.x == 0) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(&s_full[i], 1);
@@ -654,7 +625,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     const KTables &TG = G.T;
     const int lna = TG.lna;
     // slot s holds atom order[s]; slots past the ligand are padding atoms
-    // (all-zero table row, no charge; placed on the warp's first atom)
+    // (all-zero table row, no charge, far from everything)
     for (int s = threadIdx.x; s < MAXA; s += blockDim.x) {
       const int a = s < lna ? TG.lig_order[s] : -1;
       s_atom[s] = a;
@@ -874,12 +845,8 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per slot
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
-      // padding slots sit on this warp's first atom (or the ligand centre):
-      // their table rows and charges are zero, so they add exactly zero, and
-      // they change neither the close-range votes nor the denominators'
-      // range
-      const float4 o = (k < n_my) ? orig[s_atom[ag + A * k]]
-                                  : (n_my > 0 ? orig[s_atom[ag]] : make_float4(0.f, 0.f, 0.f, 0.f));
+      const float4 o =
+          (k < n_my) ? orig[s_atom[ag + A * k]] : make_float4(FAR, FAR, FAR, 0.f);
       const float x = q00 * o.x + q01 * o.y + q02 * o.z + t0 + lcx;
       const float y = q10 * o.x + q11 * o.y + q12 * o.z + t1 + lcy;
       const float z = q20 * o.x + q21 * o.y + q22 * o.z + t2 + lcz;
@@ -1107,6 +1074,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   // a split CTA leaves only when no other CTA of its cluster can still read
   // its exchange buffers
   if (csize > 1) cluster_sync_all();
+  if (R.busy_ns) {  // the CTA's time on its SM, for occupancy statistics
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(R.busy_ns, global_ns() - t_start);
+  }
 }
 
 // Temperature exchange, one thread per (item, protein conf, ligand conf)

@@ -139,6 +139,8 @@ struct gd_server {
   // error words of the lanes (device, zeroed) and their pinned host copies,
   // allocated once with the server
   int *d_err_pool = nullptr, *h_err_pool = nullptr;
+  // nanoseconds the server's CTAs spent on their SMs (all launches)
+  unsigned long long *d_busy_ns = nullptr;
 };
 
 namespace {
@@ -361,6 +363,7 @@ gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int m
   R.n_steps = 0;  // per item (item_step)
   R.item_step = 1;
   R.err = L.d_err;
+  R.busy_ns = S->d_busy_ns;
   R.split = L.split;
   for (const Req *r : rs) R.hb_pairs = std::max(R.hb_pairs, hb_pairs_of(r->item.T, L.tile.A));
   GD_CUDA(launch_dock(R, L.tile.NA, (int)n_cta * L.split, s));
@@ -663,8 +666,11 @@ extern "C" gd_status gd_server_create(int device, size_t hbm_budget_bytes, int m
   S->steps_per_launch = steps_per_launch;
   if (cudaMalloc(&S->d_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess ||
       cudaMemset(S->d_err_pool, 0, kMaxLanes * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&S->d_busy_ns, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemset(S->d_busy_ns, 0, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMallocHost(&S->h_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess) {
     if (S->d_err_pool) cudaFree(S->d_err_pool);
+    if (S->d_busy_ns) cudaFree(S->d_busy_ns);
     ctx_release(ctx);
     delete S;
     return fail(GD_ENOMEM, "server error words");
@@ -821,6 +827,8 @@ extern "C" gd_status gd_server_cancel(gd_server *S, uint64_t req_id) {
   return GD_OK;
 }
 
+extern "C" gd_ctx *gd_server_context(gd_server *S) { return S ? S->ctx : nullptr; }
+
 extern "C" gd_status gd_server_get_stats(gd_server *S, gd_server_stats *out) {
   if (!S || !out) return fail(GD_EINVAL, "gd_server_get_stats: NULL argument");
   std::lock_guard<std::mutex> g(S->mu);
@@ -831,6 +839,10 @@ extern "C" gd_status gd_server_get_stats(gd_server *S, gd_server_stats *out) {
   out->launches = S->n_launch;
   out->bytes_in_use = S->bytes_in_use + S->protein_bytes;
   out->busy_s = S->busy_s;
+  unsigned long long ns = 0;
+  cudaSetDevice(S->ctx->device);
+  GD_CUDA(cudaMemcpy(&ns, S->d_busy_ns, sizeof ns, cudaMemcpyDeviceToHost));
+  out->cta_busy_s = (double)ns * 1e-9;
   return GD_OK;
 }
 
@@ -857,6 +869,7 @@ extern "C" gd_status gd_server_destroy(gd_server *S) {
     cudaStreamDestroy(L.stream);
   }
   if (S->d_err_pool) cudaFree(S->d_err_pool);
+  if (S->d_busy_ns) cudaFree(S->d_busy_ns);
   if (S->h_err_pool) cudaFreeHost(S->h_err_pool);
   ctx_release(S->ctx);
   delete S;

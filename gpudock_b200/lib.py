@@ -83,6 +83,7 @@ def _declare(lib):
         "gd_server_cancel": ([P, C.c_uint64], i32),
         "gd_server_get_stats": ([P, C.POINTER(abi.GdServerStats)], i32),
         "gd_server_destroy": ([P], i32),
+        "gd_server_context": ([P], P),
         "gd_complex_free": ([P], i32),
         "gd_complex_device_bytes": ([P], C.c_size_t),
         "gd_energy_poses_dev": ([P, P, i32, i32, i32, P, P, P], i32),
@@ -509,6 +510,12 @@ class Server:
 
     def cancel(self, rid: int):
         check(self._lib.gd_server_cancel(self.h, C.c_uint64(rid)), "gd_server_cancel")
+
+    def set_split(self, split: int):
+        """CTAs per request unit for requests admitted from now on (0: the
+        server's rule), through the server's own context."""
+        check(self._lib.gd_ctx_set_split(self._lib.gd_server_context(self.h), split),
+              "gd_ctx_set_split")
 
     def stats(self) -> abi.GdServerStats:
         s = abi.GdServerStats()

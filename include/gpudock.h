@@ -606,6 +606,8 @@ typedef struct gd_server_stats {
   uint64_t launches;        /* kernel launches issued                       */
   size_t bytes_in_use;      /* device bytes held (proteins + requests)      */
   double busy_s;            /* seconds the scheduler spent in iterations    */
+  double cta_busy_s;        /* seconds the server's CTAs spent on SMs,      */
+                            /* summed over CTAs (/ SMs / wall = occupancy)  */
 } gd_server_stats;
 
 /* max_active <= 0 means two requests per SM. */
@@ -629,6 +631,10 @@ gd_status gd_server_wait(gd_server *srv, uint64_t req_id, int timeout_ms,
                          gd_mc_log *log);
 gd_status gd_server_cancel(gd_server *srv, uint64_t req_id);
 gd_status gd_server_get_stats(gd_server *srv, gd_server_stats *out);
+/* The server's own context (owned by the server; do not destroy it).  Its
+ * launch shapes (gd_autotune, gd_ctx_set_tile) and split rule
+ * (gd_ctx_set_split) apply to requests admitted after the call. */
+gd_ctx *gd_server_context(gd_server *srv);
 gd_status gd_server_destroy(gd_server *srv);
 
 /* ------------------------------------------------------------------------ */

@@ -139,8 +139,8 @@ def test_plain_config_statistics(ctx):
     att = exchange_attempts(steps, spe, n_tmp)
     assert 0 < gs.sum() < att * len(gs) and 0 < cs.sum() < att * len(cs)
     p_swap = stats.ttest_ind(gs, cs, equal_var=False).pvalue
-    tot = len(gs) * att
-    p_fisher = stats.fisher_exact([[gs.sum(), tot - gs.sum()], [cs.sum(), tot - cs.sum()]]).pvalue
+    tg, tc = len(gs) * att, len(cs) * att  # attempts of each side
+    p_fisher = stats.fisher_exact([[gs.sum(), tg - gs.sum()], [cs.sum(), tc - cs.sum()]]).pvalue
     _family([p_swap, p_fisher], "swaps per group (Welch) and pooled (Fisher)")
     # acceptance rises with the temperature (slot 0 is the lowest)
     assert np.all(np.diff(ga.mean(axis=0)) >= -0.02)
