@@ -34,10 +34,11 @@ constexpr uint32_t META_SEQ_SHIFT = 12u;
 constexpr int MAX_SEQ3R = (1 << 20) - 1;
 // Points past the protein's last point (up to the tile boundary) are padding:
 // type PAD_POINT_TYPE, whose kernel table rows are all zero, no charge, and
-// far from everything (on the opposite side from the padding ligand atoms),
-// so the pair loop may run over them and add exactly zero.
+// far from everything (on the opposite side from the padding ligand atoms,
+// with d^9 to any atom still finite in FP32), so the pair loop may run over
+// them and add exactly zero.
 constexpr int PAD_POINT_TYPE = 31;
-constexpr float PAD_POINT_COORD = -1.0e4f;
+constexpr float PAD_POINT_COORD = -3.0e3f;
 
 enum KMode : int { KMODE_POSES = 0, KMODE_REMC = 1, KMODE_INIT = 2 };
 

@@ -43,7 +43,9 @@ constexpr int STAGE_BYTES = TILE_PTS * (16 + 8);
 constexpr int CHUNK = 32;  // points per FP32 partial before the FP64 flush
 constexpr int kPointUnroll = 2;  // protein points per iteration of the fast path
 constexpr float LOG2E = 1.4426950408889634f;
-constexpr float FAR = 1.0e4f;  // coordinate of the padding atoms
+// coordinate of the padding atoms: far from every point, and close enough
+// that d^9 to any point stays finite in FP32
+constexpr float FAR = 1.0e3f;
 // Point types of the kernel's pair tables: the force field's GD_NPT plus
 // all-zero rows, one of which (PAD_POINT_TYPE) marks the padding points that
 // fill a tile past the protein's last point, so they add exactly zero.
@@ -379,9 +381,16 @@ struct PairConst {
 // sums of ele/d), contact PMF and, for the first NHB atom pairs, the H-bond
 // term (H-bond-capable atoms come first in the slot order, so the later
 // pairs of a warp have none; weight 0 and hdb0 = 0 for an atom of a pair
-// without it).  The LJ and PMF quotients share one reciprocal: with D1 = p4
-// and D2 = 1 + exp(.), num1/D1 = num1 D2 / (D1 D2).  pp / hp point at the
-// point type's entry of atom pair 0 of this warp's pair tables.
+// without it).  pp / hp point at the point type's entry of atom pair 0 of
+// this warp's pair tables.
+//
+// The soft LJ of calcenergy_d.cu:96-100, (p1 - p2) / p4 with p1 = p1a / d^9,
+// p2 = p2a / d^6, p4 = 1 + p1 L and L = lj0 (1 + lj1 d^2), is evaluated
+// multiplied through by d^9: (p1a - p2a d^3) / (d^9 + p1a L).  That takes
+// two multiplies fewer than the powers of 1/d, and its denominator D1 stays
+// between p1a L and d^9, so it cannot overflow at short range.  The LJ and
+// PMF quotients share one reciprocal: with D2 = 1 + exp(.),
+// num1/D1 = num1 D2 / (D1 D2) and pmf1/D2 = pmf1 D1 / (D1 D2).
 // Branch-free and written in stages over all atom pairs -- distances and
 // rsqrt, then powers, PMF argument and exp, then the shared reciprocals and
 // sums, then the H-bond Gaussians -- so that the MUFU operations of one
@@ -402,29 +411,26 @@ __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2
     d2[h] = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
     r[h] = make_float2(frsqrt(d2[h].x), frsqrt(d2[h].y));
   }
-  float2 ex[NH], p4[NH], p12[NH], pm[NH];
+  float2 ex[NH], den1[NH], num1[NH], pm[NH];
 #pragma unroll
   for (int h = 0; h < NH; ++h) {
     const float4 T0 = pp[h * 2 * PT_ROWS];      // p1a, -p2a
     const float4 T1 = pp[h * 2 * PT_ROWS + 1];  // -pmf0, pmf1
     const float2 d = mul2(d2[h], r[h]);
-    const float2 r2 = mul2(r[h], r[h]);
-    const float2 r3 = mul2(r2, r[h]);
-    const float2 r6 = mul2(r3, r3);
-    const float2 t9 = mul2(lo2(T0), r3);  // p1a r^3, beside r^6
-    const float2 p1 = mul2(t9, r6);
-    p12[h] = fma2(hi2(T0), r6, p1);  // p1 - p2
-    p4[h] = fma2(p1, fma2(K.lj1, d2[h], K.lj0), K.one);
-    pm[h] = mul2(hi2(T1), p4[h]);
+    const float2 g = mul2(d2[h], d);            // d^3
+    const float2 g3 = mul2(mul2(g, g), g);      // d^9
+    den1[h] = fma2(lo2(T0), fma2(K.lj1, d2[h], K.lj0), g3);  // d^9 + p1a L
+    num1[h] = fma2(hi2(T0), g, lo2(T0));                      // p1a - p2a d^3
+    pm[h] = mul2(hi2(T1), den1[h]);
     const float2 arg = mul2(fma2(K.ca, d, K.cb), add2(d, lo2(T1)));
     ex[h] = make_float2(fex2(arg.x), fex2(arg.y));
   }
 #pragma unroll
   for (int h = 0; h < NH; ++h) {
-    // D1 D2 and num1 D2 as single FMAs: p4 (1 + ex) = p4 ex + p4
-    const float2 den = fma2(p4[h], ex[h], p4[h]);
+    // D1 D2 and num1 D2 as single FMAs: D1 (1 + ex) = D1 ex + D1
+    const float2 den = fma2(den1[h], ex[h], den1[h]);
     const float2 inv = make_float2(frcp(den.x), frcp(den.y));
-    fvdw = fma2(fma2(p12[h], ex[h], p12[h]), inv, fvdw);
+    fvdw = fma2(fma2(num1[h], ex[h], num1[h]), inv, fvdw);
     fpmf = fma2(pm[h], inv, fpmf);
     fek[h] = fma2(dup2(A0.w), r[h], fek[h]);
     mn = fminf(mn, fminf(d2[h].x, d2[h].y));
@@ -439,11 +445,6 @@ __device__ __forceinline__ void pair_block1(const float2 (&nx)[NH], const float2
   }
 }
 
-// The fast path over points j0 .. j1-1 of a staged tile, one point per
-// iteration and no branch in the body, so the compiler can overlap one
-// point's tail with the next point's head.  Returns the mask of points whose
-// close-range terms must run: some lane has an atom within the point's
-// threshold (thr_l, held by lane j - j0).  NHB: atom pairs with the H-bond term.
 template <int NH, int NHB>
 __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const float2 (&ny)[NH],
                                                const float2 (&nz)[NH], const float4 *ta,
