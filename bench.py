@@ -458,6 +458,8 @@ def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool
            "p99_service_s": float(np.percentile(svc[skip:], 99)),
            "latency_window": f"requests {skip}..{n_request - 1} (after the first fifth)",
            "sm_occupancy": st.cta_busy_s / (n_sm * wall),
+           "lane_run_s": st.lane_run_s, "lane_gap_s": st.lane_gap_s,
+           "host_launch_s": st.host_launch_s,
            "busy_s": st.busy_s, "launches": st.launches,
            "queue_series": {"every_s": 0.5, "columns": ["t_s", "queued", "active", "completed"],
                             "rows": series[::4]},

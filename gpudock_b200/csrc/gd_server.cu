@@ -16,6 +16,7 @@
 // There is no counterpart in the reference (Run() handles one complex per
 // process, run.cu:41-353); the semantics of every request are those of Run.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -96,6 +97,10 @@ struct Lane {
   int split = 1;                    // CTAs (a cluster) per request unit
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  // timing events around each launch: the run time of the lane's launches
+  // and the gaps between them on the GPU's clock (statistics)
+  cudaEvent_t t_start = nullptr, t_end = nullptr, t_end_prev = nullptr;
+  bool have_prev = false;
   int *d_err = nullptr;             // the lane's kernel error word
   int *h_err = nullptr;             // pinned copy, read after `done`
   bool busy = false;                // a launch is in flight
@@ -141,6 +146,10 @@ struct gd_server {
   int *d_err_pool = nullptr, *h_err_pool = nullptr;
   // nanoseconds the server's CTAs spent on their SMs (all launches)
   unsigned long long *d_busy_ns = nullptr;
+  // lanes' launch run time and the gaps between a lane's launches (GPU
+  // clock), and the scheduler thread's time spent issuing launches
+  // (written by the scheduler thread only, read by gd_server_get_stats)
+  std::atomic<double> lane_run_s{0.0}, lane_gap_s{0.0}, host_launch_s{0.0};
 };
 
 namespace {
@@ -226,6 +235,9 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d launch shapes in the server", kMaxLanes);
   GD_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
   GD_CUDA(cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming));
+  GD_CUDA(cudaEventCreate(&L->t_start));
+  GD_CUDA(cudaEventCreate(&L->t_end));
+  GD_CUDA(cudaEventCreate(&L->t_end_prev));
   L->d_err = S->d_err_pool + slot;
   L->h_err = S->h_err_pool + slot;
   *out = L.get();
@@ -507,6 +519,15 @@ void scheduler(gd_server *S) {
         if (q == cudaErrorNotReady) continue;
         L.busy = false;
         progressed = true;
+        {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, L.t_start, L.t_end) == cudaSuccess)
+            S->lane_run_s.store(S->lane_run_s.load() + ms * 1e-3);
+          if (L.have_prev && cudaEventElapsedTime(&ms, L.t_end_prev, L.t_start) == cudaSuccess)
+            S->lane_gap_s.store(S->lane_gap_s.load() + ms * 1e-3);
+          std::swap(L.t_end, L.t_end_prev);
+          L.have_prev = true;
+        }
         gd_status st = GD_OK;
         if (q != cudaSuccess) {
           st = fail(GD_ECUDA, "server launch: %s", cudaGetErrorString(q));
@@ -555,7 +576,10 @@ void scheduler(gd_server *S) {
     for (auto &kv : S->lanes) {
       Lane &L = *kv.second;
       if (L.busy || (L.members.empty() && L.fresh.empty())) continue;
-      gd_status st = GD_OK;
+      const auto t_issue = Clock::now();
+      gd_status st = cudaEventRecord(L.t_start, L.stream) == cudaSuccess
+                         ? GD_OK
+                         : fail(GD_ECUDA, "server: event record");
       if (!L.fresh.empty()) {
         st = launch_lane(S, L, L.fresh, KMODE_INIT);
         for (Req *r : L.fresh) L.members.push_back(r);
@@ -565,6 +589,8 @@ void scheduler(gd_server *S) {
         plan_steps(S, L.members);
         st = launch_lane(S, L, L.members, KMODE_REMC);
       }
+      if (st == GD_OK && cudaEventRecord(L.t_end, L.stream) != cudaSuccess)
+        st = fail(GD_ECUDA, "server: event record");
       if (st == GD_OK && cudaMemcpyAsync(L.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost,
                                          L.stream) != cudaSuccess)
         st = fail(GD_ECUDA, "server: error word copy");
@@ -576,6 +602,8 @@ void scheduler(gd_server *S) {
         L.members.clear();
         continue;
       }
+      S->host_launch_s.store(S->host_launch_s.load() +
+                             std::chrono::duration<double>(Clock::now() - t_issue).count());
       L.in_flight = L.members;
       L.busy = true;
       S->n_iter += 1;
@@ -843,6 +871,9 @@ extern "C" gd_status gd_server_get_stats(gd_server *S, gd_server_stats *out) {
   cudaSetDevice(S->ctx->device);
   GD_CUDA(cudaMemcpy(&ns, S->d_busy_ns, sizeof ns, cudaMemcpyDeviceToHost));
   out->cta_busy_s = (double)ns * 1e-9;
+  out->lane_run_s = S->lane_run_s.load();
+  out->lane_gap_s = S->lane_gap_s.load();
+  out->host_launch_s = S->host_launch_s.load();
   return GD_OK;
 }
 
@@ -866,6 +897,9 @@ extern "C" gd_status gd_server_destroy(gd_server *S) {
     if (L.d_cta) cudaFree(L.d_cta);
     if (L.d_groups) cudaFree(L.d_groups);
     cudaEventDestroy(L.done);
+    cudaEventDestroy(L.t_start);
+    cudaEventDestroy(L.t_end);
+    cudaEventDestroy(L.t_end_prev);
     cudaStreamDestroy(L.stream);
   }
   if (S->d_err_pool) cudaFree(S->d_err_pool);
