@@ -43,6 +43,11 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The serving form runs one stream per launch shape; with the driver's
+# default of 8 hardware work queues, launches of unrelated streams that map
+# to one queue wait for each other.  32 queues (the maximum) must be asked
+# for before the CUDA context exists.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 FLOP_PER_PAIR = 36  # algorithmic FP32 flops per ligand-protein pair
 
@@ -458,7 +463,6 @@ def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool
            "p99_service_s": float(np.percentile(svc[skip:], 99)),
            "latency_window": f"requests {skip}..{n_request - 1} (after the first fifth)",
            "sm_occupancy": st.cta_busy_s / (n_sm * wall),
-           "lane_run_s": st.lane_run_s, "lane_gap_s": st.lane_gap_s,
            "host_launch_s": st.host_launch_s,
            "busy_s": st.busy_s, "launches": st.launches,
            "queue_series": {"every_s": 0.5, "columns": ["t_s", "queued", "active", "completed"],

@@ -128,8 +128,7 @@ class GdServerStats(C.Structure):
     _fields_ = [
         ("queued", C.c_int), ("active", C.c_int), ("completed", C.c_uint64),
         ("iterations", C.c_uint64), ("launches", C.c_uint64), ("bytes_in_use", C.c_size_t),
-        ("busy_s", C.c_double), ("cta_busy_s", C.c_double), ("lane_run_s", C.c_double),
-        ("lane_gap_s", C.c_double), ("host_launch_s", C.c_double),
+        ("busy_s", C.c_double), ("cta_busy_s", C.c_double), ("host_launch_s", C.c_double),
     ]
 
 

@@ -560,6 +560,19 @@ static gd_status upload_ligand(const gd_complex *cx, gd_dcomplex *d) {
   GD_TRY(upload(d, lt, &T.lig_t));
   GD_TRY(upload(d, lq, &T.lig_q));
   GD_TRY(upload(d, psp, &T.psp));
+  {
+    // residues where some atom type of this ligand has a nonzero psp entry:
+    // the kernel reads the table only there (elsewhere it adds zero)
+    const int n_col = cx->psp.n_col;
+    bool present[GD_NLT] = {};
+    for (int a = 0; a < lna; ++a) present[L.t[a]] = true;
+    std::vector<uint32_t> mask((size_t)(n_col + 31) / 32, 0u);
+    for (int t = 0; t < GD_NLT; ++t)
+      if (present[t])
+        for (int r = 0; r < n_col; ++r)
+          if (psp[(size_t)t * n_col + r] != 0.0f) mask[r >> 5] |= 1u << (r & 31);
+    GD_TRY(upload(d, mask, &T.psp_mask));
+  }
   GD_TRY(upload(d, kd, &T.kde));
   GD_TRY(upload(d, koff, &T.kde_off));
   GD_TRY(upload(d, mc, &T.mcs));

@@ -54,6 +54,8 @@ struct KTables {
   const int *lig_t;     // [lna]
   const float *lig_q;   // [lna]
   const float *psp;     // [NLT][psp_ncol]
+  const uint32_t *psp_mask;  // [(psp_ncol + 31) / 32] bit r: some atom type of
+                             // this ligand has a nonzero psp[type][r]
   const float4 *kde;    // [pnk] sorted by type {x, y, z, 0}
   const int *kde_off;   // [NLT + 1]
   const float4 *mcs;    // [pos][lna] {x, y, z, valid}

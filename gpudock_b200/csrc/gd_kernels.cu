@@ -177,17 +177,6 @@ __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); 
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
-// Hydrophobic contact polynomial of calcenergy_d.cu:80-86 in Horner form:
-// 1 - (3.5/81 d2 - 4.5/81^2 d4 + 2.5/81^3 d6 - 0.5/81^4 d8)
-__device__ __forceinline__ float hpc_poly(float d2) {
-  const float c1 = 3.5f / 81.0f;
-  const float c2 = -4.5f / 81.0f / 81.0f;
-  const float c3 = 2.5f / 81.0f / 81.0f / 81.0f;
-  const float c4 = -0.5f / 81.0f / 81.0f / 81.0f / 81.0f;
-  const float q = fmaf(fmaf(fmaf(c4, d2, c3), d2, c2), d2, c1);
-  return 1.0f - q * d2;
-}
-
 // ZYX Euler rotation of move_d.cu:90-105 (row-major 3x3).
 __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R) {
   float s1, c1, s2, c2, s3, c3;
@@ -205,6 +194,15 @@ __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R)
   R[8] = c2 * c3;
 }
 
+// Per-atom hydrophobic sums in shared memory: for tile group g, the float2
+// of atom pair h (slots ag + 2hA, ag + (2h+1)A) of atom group ag and lane
+// `lane` sits at float2 index ((g A + ag) NH + h) 32 + lane.  Index of the
+// float of slot a:
+__device__ __forceinline__ int hpc_at(int g, int a, int lane, int A, int NH) {
+  const int ag = a % A, k = a / A;
+  return ((((g * A + ag) * NH + (k >> 1)) * 32 + lane) << 1) + (k & 1);
+}
+
 // Warp 0 after the step's partial sums: cross-warp reduction in a fixed
 // order, hydrophobic transform per atom, normalisation and total in the
 // reference's order, then the pose output, or the Metropolis decision (with
@@ -214,8 +212,9 @@ __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R)
 template <int MODE>
 __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneState &me,
                                          double *s_red, const float *s_hpc, const int *s_lt,
-                                         int W, int P, int MAXA, int lane, int rep, bool active,
-                                         int prt_conf, int lig_conf, int step, bool primary) {
+                                         int W, int P, int A, int NH, int lane, int rep,
+                                         bool active, int prt_conf, int lig_conf, int step,
+                                         bool primary) {
   const KTables &T = I.T;
   const int lna = T.lna;
   const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
@@ -231,7 +230,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
     // slot (slot a holds one atom, s_lt its type)
     for (int a = 0; a < lna; ++a) {
       float h = 0.f;
-      for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
+      for (int g = 0; g < P; ++g) h += s_hpc[hpc_at(g, a, lane, A, NH)];
       const int lt = s_lt[a];
       const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
       S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
@@ -479,22 +478,32 @@ __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const flo
 // of every point, counted (with those also in the reference map,
 // calcmcc_d.cu:148-213) straight into the lane's FP64 slots 8 and 9 of
 // my_red, so the rare counts hold no registers in the pair loop.  Distances
-// are recomputed per atom; p is the point's index in the protein.
+// are recomputed per atom pair; p is the point's index in the protein.
+// The hydrophobic polynomial runs packed over an atom pair, branch-free
+// (zero beyond 9 A and for padding slots), into the pair's float2 of
+// per-atom sums (my_hpc2 + 32 h).  The PSP table is read only for residues
+// where some atom type of this ligand has a nonzero entry (T.psp_mask): the
+// others would add exactly zero.
 template <int NA>
 __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const float2 (&ny)[NA / 2],
                                             const float2 (&nz)[NA / 2], const float4 &Ap,
                                             float hpp, uint32_t meta, const float4 *pp,
                                             const KTables &T, const float *s_q, const int *s_lt,
-                                            const int *s_atom, float *my_hpc, int A, int ag,
+                                            const int *s_atom, float2 *my_hpc2, int A, int ag,
                                             int n_my, float inv_el1, float &fnear, float &fpsp,
                                             bool mcc_on, int p, double *my_red) {
   const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
   const bool hflag = (meta & META_HPC_BIT) != 0u;
+  const uint32_t res = meta >> META_SEQ_SHIFT;
+  const bool psp_on = is_c2 && ((__ldg(&T.psp_mask[res >> 5]) >> (res & 31)) & 1u) != 0u;
+  const bool pm_on = psp_on || mcc_on;  // the d <= pmf0 block below
   // the largest squared distance at which a term below can fire for this
-  // point: atom pairs that no lane has within it are skipped (warp-uniform);
-  // in practice a few percent of a close point's atom pairs are in range
-  const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f,
-                                             (is_c2 || mcc_on) ? T.near_mcc2 : 0.0f));
+  // point: atom pairs that no lane has within it are skipped (warp-uniform)
+  const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f, pm_on ? T.near_mcc2 : 0.0f));
+  const float c1 = 3.5f / 81.0f;
+  const float c2 = -4.5f / 81.0f / 81.0f;
+  const float c3 = 2.5f / 81.0f / 81.0f / 81.0f;
+  const float c4 = -0.5f / 81.0f / 81.0f / 81.0f / 81.0f;
 #pragma unroll
   for (int h = 0; h < NA / 2; ++h) {
     const float2 dx2 = add2(nx[h], dup2(Ap.x));
@@ -502,14 +511,18 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
     const float2 dz2 = add2(nz[h], dup2(Ap.z));
     const float2 d2p = fma2(dx2, dx2, fma2(dy2, dy2, mul2(dz2, dz2)));
     if (!__any_sync(0xffffffffu, fminf(d2p.x, d2p.y) <= thr)) continue;
+    if (hflag) {
+      // 1 - (c1 d2 + c2 d4 + c3 d6 + c4 d8), Horner in d2
+      const float2 q = fma2(fma2(fma2(dup2(c4), d2p, dup2(c3)), d2p, dup2(c2)), d2p, dup2(c1));
+      float2 poly = fma2(make_float2(-q.x, -q.y), d2p, dup2(1.0f));
+      poly.x = (d2p.x <= 81.0f && 2 * h < n_my) ? poly.x : 0.0f;
+      poly.y = (d2p.y <= 81.0f && 2 * h + 1 < n_my) ? poly.y : 0.0f;
+      my_hpc2[h * 32] = fma2(dup2(hpp), poly, my_hpc2[h * 32]);
+    }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int k = 2 * h + j;
       const float d2 = j ? d2p.y : d2p.x;
-      if (hflag && d2 <= 81.0f && k < n_my) {
-        float *hh = my_hpc + (size_t)A * k * 32;
-        *hh = fmaf(hpp, hpc_poly(d2), *hh);
-      }
       // the distance itself only where a switch can be near (d^2 bounds with
       // margin: the tests below decide on d exactly as before)
       if (d2 <= T.near_ele2) {
@@ -520,13 +533,12 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
           fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
         }
       }
-      if ((is_c2 || mcc_on) && k < n_my && d2 <= T.near_mcc2) {
+      if (pm_on && k < n_my && d2 <= T.near_mcc2) {
         const float d = d2 * frsqrt(d2);
         const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
         const float dm = d + ((k & 1) ? T1.y : T1.x);
         if (dm <= 0.0f) {
-          if (is_c2)
-            fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + (meta >> META_SEQ_SHIFT)]);
+          if (psp_on) fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + res]);
           if (mcc_on) {
             const int a = s_atom[ag + A * k];
             my_red[8 * 32] += 1.0;
@@ -619,11 +631,13 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   // ---- item of this piece into shared memory, pair tables -----------------
   const int item = (MODE == KMODE_POSES) ? 0 : R.cta_item[unit];
   if (item != s_ctl->item) {
-    const KItem &G = R.items[item];
-    const uint32_t *src = reinterpret_cast<const uint32_t *>(&G);
+    // one read of the descriptor (it may live in pinned host memory), then
+    // the shared-memory copy
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&R.items[item]);
     uint32_t *dst = reinterpret_cast<uint32_t *>(s_item);
     for (int i = threadIdx.x; i < (int)(sizeof(KItem) / 4); i += blockDim.x) dst[i] = src[i];
-    const KTables &TG = G.T;
+    __syncthreads();
+    const KTables &TG = s_item->T;
     const int lna = TG.lna;
     // slot s holds atom order[s]; slots past the ligand are padding atoms
     // (all-zero table row, no charge, far from everything)
@@ -843,7 +857,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     float2 nx[NH], ny[NH], nz[NH];
     // per-atom hydrophobic sums of this warp's tiles live in shared memory
     // (touched only on the close-range path)
-    float *my_hpc = s_hpc + ((size_t)pg * MAXA + ag) * 32 + lane;  // + A*k*32 per slot
+    float2 *my_hpc2 = reinterpret_cast<float2 *>(s_hpc) + (size_t)(pg * A + ag) * NH * 32 + lane;
 #pragma unroll
     for (int k = 0; k < NA; ++k) {
       const float4 o =
@@ -860,8 +874,9 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         ny[k >> 1].x = -y;
         nz[k >> 1].x = -z;
       }
-      if (k < n_my) my_hpc[(size_t)A * k * 32] = 0.f;
     }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) my_hpc2[h * 32] = make_float2(0.f, 0.f);
 
     // ---- pair terms over the protein tiles -----------------------------------
     // FP64 sums of this lane live in the warp's own reduction slots (read by
@@ -919,7 +934,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
           const uint32_t meta = __float_as_uint(tb[j].y);
           close_range<NA>(nx, ny, nz, ta[j], tb[j].x, meta,
                           my_ptab + (int)(meta & META_TYPE_MASK) * 2, T, s_q, s_lt, s_atom,
-                          my_hpc, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
+                          my_hpc2, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
                           my_red);
         }
         float fele = 0.f;
@@ -1016,7 +1031,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         }
         for (int a = 0; a < lna; ++a) {
           float h = 0.f;
-          for (int g = 0; g < P; ++g) h += s_hpc[((size_t)g * MAXA + a) * 32 + lane];
+          for (int g = 0; g < P; ++g) h += s_hpc[hpc_at(g, a, lane, A, NH)];
           xh[a * 32 + lane] = h;
         }
       }
@@ -1030,13 +1045,13 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         for (int a = 0; a < lna; ++a) {
           float h = 0.f;
           for (int r = 0; r < csize; ++r) h += cluster_map(xh, r)[a * 32 + lane];
-          s_hpc[(size_t)a * 32 + lane] = h;  // tile group 0's slots
+          s_hpc[hpc_at(0, a, lane, A, NH)] = h;  // tile group 0's slots
         }
-        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, MAXA, lane, rep, active, prt_conf,
+        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, A, NH, lane, rep, active, prt_conf,
                           lig_conf, step, crank0 == 0);
       }
     } else if (warp == 0) {
-      finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, MAXA, lane, rep, active, prt_conf,
+      finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, A, NH, lane, rep, active, prt_conf,
                         lig_conf, step, true);
     }
     // the next step's first barrier orders warp 0's updates (and its use of

@@ -97,21 +97,24 @@ struct Lane {
   int split = 1;                    // CTAs (a cluster) per request unit
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
-  // timing events around each launch: the run time of the lane's launches
-  // and the gaps between them on the GPU's clock (statistics)
-  cudaEvent_t t_start = nullptr, t_end = nullptr, t_end_prev = nullptr;
-  bool have_prev = false;
-  int *d_err = nullptr;             // the lane's kernel error word
-  int *h_err = nullptr;             // pinned copy, read after `done`
+  // the lane's kernel error word, in pinned host memory the kernels write
+  // directly (read after `done`)
+  int *h_err = nullptr;
   bool busy = false;                // a launch is in flight
   std::vector<Req *> members;       // active requests of this shape
   std::vector<Req *> fresh;         // admitted, not yet initialised
   std::vector<Req *> in_flight;     // the requests of the launch in flight
-  // launch descriptors, grown on demand (reused: one launch at a time)
-  KItem *d_items = nullptr;
-  int *d_cta = nullptr;  // [3][cap_cta]
-  KGroup *d_groups = nullptr;
-  size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
+  // Launch descriptors in pinned host memory that the kernels read directly
+  // (no copy in the lane's stream, so a launch is one or two kernels and an
+  // event): one set for the INIT launch and one for the MC launch that
+  // follows it on the stream.  A set is rewritten only when the lane's
+  // previous launch has ended.
+  struct Desc {
+    KItem *items = nullptr;
+    int *cta = nullptr;  // [3][cap_cta]
+    KGroup *groups = nullptr;
+    size_t cap_items = 0, cap_cta = 0, cap_groups = 0;
+  } desc[2];
 };
 
 using LaneKey = std::tuple<int, int, int, int, int, int, int, int>;
@@ -143,13 +146,12 @@ struct gd_server {
   std::map<LaneKey, std::unique_ptr<Lane>> lanes;
   // error words of the lanes (device, zeroed) and their pinned host copies,
   // allocated once with the server
-  int *d_err_pool = nullptr, *h_err_pool = nullptr;
+  int *h_err_pool = nullptr;  // lanes' error words (pinned, written by kernels)
   // nanoseconds the server's CTAs spent on their SMs (all launches)
   unsigned long long *d_busy_ns = nullptr;
-  // lanes' launch run time and the gaps between a lane's launches (GPU
-  // clock), and the scheduler thread's time spent issuing launches
-  // (written by the scheduler thread only, read by gd_server_get_stats)
-  std::atomic<double> lane_run_s{0.0}, lane_gap_s{0.0}, host_launch_s{0.0};
+  // the scheduler thread's time spent issuing launches (written by the
+  // scheduler thread only, read by gd_server_get_stats)
+  std::atomic<double> host_launch_s{0.0};
 };
 
 namespace {
@@ -194,15 +196,15 @@ void release_device(Req *r) {
   }
 }
 
-// Grows a lane's descriptor buffer in stream order on the lane's stream (no
-// device-wide synchronisation while other lanes run).
+// Grows a lane's pinned descriptor buffer (only while the lane is idle).
 template <typename T>
-gd_status grow(T **p, size_t *cap, size_t need, cudaStream_t s) {
+gd_status grow(T **p, size_t *cap, size_t need) {
   if (need <= *cap) return GD_OK;
   size_t n = std::max<size_t>(need, *cap * 2 + 64);
-  if (*p) cudaFreeAsync(*p, s);
+  if (*p) cudaFreeHost(*p);
   *p = nullptr;
-  GD_CUDA(cudaMallocAsync((void **)p, n * sizeof(T), s));
+  *cap = 0;
+  GD_CUDA(cudaMallocHost((void **)p, n * sizeof(T)));
   *cap = n;
   return GD_OK;
 }
@@ -235,10 +237,6 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d launch shapes in the server", kMaxLanes);
   GD_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
   GD_CUDA(cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming));
-  GD_CUDA(cudaEventCreate(&L->t_start));
-  GD_CUDA(cudaEventCreate(&L->t_end));
-  GD_CUDA(cudaEventCreate(&L->t_end_prev));
-  L->d_err = S->d_err_pool + slot;
   L->h_err = S->h_err_pool + slot;
   *out = L.get();
   S->lanes[key] = std::move(L);
@@ -340,41 +338,35 @@ gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int m
   std::stable_sort(ctas.begin(), ctas.end(),
                    [](const auto &a, const auto &b) { return std::get<0>(a) > std::get<0>(b); });
   const size_t n_cta = ctas.size();
-  GD_TRY(grow(&L.d_items, &L.cap_items, items.size(), s));
-  GD_TRY(grow(&L.d_cta, &L.cap_cta, 3 * n_cta, s));
-  GD_TRY(grow(&L.d_groups, &L.cap_groups, std::max<size_t>(groups.size(), 1), s));
-  std::vector<int> cta(3 * n_cta);
+  // the lane's previous launch has ended, so its descriptor set is free
+  Lane::Desc &D = L.desc[mode == KMODE_INIT ? 0 : 1];
+  GD_TRY(grow(&D.items, &D.cap_items, items.size()));
+  GD_TRY(grow(&D.cta, &D.cap_cta, 3 * n_cta));
+  GD_TRY(grow(&D.groups, &D.cap_groups, std::max<size_t>(groups.size(), 1)));
+  std::memcpy(D.items, items.data(), items.size() * sizeof(KItem));
   for (size_t c = 0; c < n_cta; ++c) {
-    cta[c] = std::get<1>(ctas[c]);
-    cta[n_cta + c] = std::get<2>(ctas[c]);
-    cta[2 * n_cta + c] = std::get<3>(ctas[c]);
+    D.cta[c] = std::get<1>(ctas[c]);
+    D.cta[n_cta + c] = std::get<2>(ctas[c]);
+    D.cta[2 * n_cta + c] = std::get<3>(ctas[c]);
   }
-  // the lane's previous launch has ended, and pageable copies stage
-  // synchronously, so the descriptors can be reused
-  GD_CUDA(cudaMemcpyAsync(L.d_items, items.data(), items.size() * sizeof(KItem),
-                          cudaMemcpyHostToDevice, s));
-  GD_CUDA(cudaMemcpyAsync(L.d_cta, cta.data(), cta.size() * sizeof(int), cudaMemcpyHostToDevice,
-                          s));
-  if (!groups.empty())
-    GD_CUDA(cudaMemcpyAsync(L.d_groups, groups.data(), groups.size() * sizeof(KGroup),
-                            cudaMemcpyHostToDevice, s));
+  if (!groups.empty()) std::memcpy(D.groups, groups.data(), groups.size() * sizeof(KGroup));
   KRun R{};
   R.mode = mode;
   R.A = L.tile.A;
   R.P = L.tile.P;
   R.n_stages = L.ns;
   R.resident = L.res;
-  R.items = L.d_items;
-  R.cta_item = L.d_cta;
-  R.cta_rep0 = L.d_cta + n_cta;
-  R.cta_nrep = L.d_cta + 2 * n_cta;
+  R.items = D.items;
+  R.cta_item = D.cta;
+  R.cta_rep0 = D.cta + n_cta;
+  R.cta_nrep = D.cta + 2 * n_cta;
   R.group_major = L.gm;
   R.fused_exchange = L.gm;
   R.spe = L.spe;
   R.step0 = 0;
   R.n_steps = 0;  // per item (item_step)
   R.item_step = 1;
-  R.err = L.d_err;
+  R.err = L.h_err;
   R.busy_ns = S->d_busy_ns;
   R.split = L.split;
   for (const Req *r : rs) R.hb_pairs = std::max(R.hb_pairs, hb_pairs_of(r->item.T, L.tile.A));
@@ -383,7 +375,7 @@ gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int m
   S->n_launch += 1;
   if (!groups.empty()) {
     // per-item mode (step0 < 0): each group uses its item's step and spe
-    GD_CUDA(launch_exchange(L.d_items, L.d_groups, (int)groups.size(), 1, -1, nullptr, s));
+    GD_CUDA(launch_exchange(D.items, D.groups, (int)groups.size(), 1, -1, nullptr, s));
     S->ctx->launches += 1;
     S->n_launch += 1;
   }
@@ -519,22 +511,12 @@ void scheduler(gd_server *S) {
         if (q == cudaErrorNotReady) continue;
         L.busy = false;
         progressed = true;
-        {
-          float ms = 0.f;
-          if (cudaEventElapsedTime(&ms, L.t_start, L.t_end) == cudaSuccess)
-            S->lane_run_s.store(S->lane_run_s.load() + ms * 1e-3);
-          if (L.have_prev && cudaEventElapsedTime(&ms, L.t_end_prev, L.t_start) == cudaSuccess)
-            S->lane_gap_s.store(S->lane_gap_s.load() + ms * 1e-3);
-          std::swap(L.t_end, L.t_end_prev);
-          L.have_prev = true;
-        }
         gd_status st = GD_OK;
         if (q != cudaSuccess) {
           st = fail(GD_ECUDA, "server launch: %s", cudaGetErrorString(q));
-        } else if (*L.h_err != 0) {
+        } else if (*(volatile int *)L.h_err != 0) {
           st = kernel_error(*L.h_err);
-          *L.h_err = 0;
-          cudaMemsetAsync(L.d_err, 0, sizeof(int), L.stream);
+          *(volatile int *)L.h_err = 0;  // the lane's next launch starts after this
         }
         for (Req *r : L.in_flight) {
           if (st != GD_OK) {
@@ -577,9 +559,7 @@ void scheduler(gd_server *S) {
       Lane &L = *kv.second;
       if (L.busy || (L.members.empty() && L.fresh.empty())) continue;
       const auto t_issue = Clock::now();
-      gd_status st = cudaEventRecord(L.t_start, L.stream) == cudaSuccess
-                         ? GD_OK
-                         : fail(GD_ECUDA, "server: event record");
+      gd_status st = GD_OK;
       if (!L.fresh.empty()) {
         st = launch_lane(S, L, L.fresh, KMODE_INIT);
         for (Req *r : L.fresh) L.members.push_back(r);
@@ -589,11 +569,6 @@ void scheduler(gd_server *S) {
         plan_steps(S, L.members);
         st = launch_lane(S, L, L.members, KMODE_REMC);
       }
-      if (st == GD_OK && cudaEventRecord(L.t_end, L.stream) != cudaSuccess)
-        st = fail(GD_ECUDA, "server: event record");
-      if (st == GD_OK && cudaMemcpyAsync(L.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost,
-                                         L.stream) != cudaSuccess)
-        st = fail(GD_ECUDA, "server: error word copy");
       if (st == GD_OK && cudaEventRecord(L.done, L.stream) != cudaSuccess)
         st = fail(GD_ECUDA, "server: event record");
       if (st != GD_OK) {
@@ -692,12 +667,9 @@ extern "C" gd_status gd_server_create(int device, size_t hbm_budget_bytes, int m
   S->budget = hbm_budget_bytes;
   S->max_active = max_active > 0 ? max_active : 2 * ctx->n_sm;
   S->steps_per_launch = steps_per_launch;
-  if (cudaMalloc(&S->d_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess ||
-      cudaMemset(S->d_err_pool, 0, kMaxLanes * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&S->d_busy_ns, sizeof(unsigned long long)) != cudaSuccess ||
+  if (cudaMalloc(&S->d_busy_ns, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMemset(S->d_busy_ns, 0, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMallocHost(&S->h_err_pool, kMaxLanes * sizeof(int)) != cudaSuccess) {
-    if (S->d_err_pool) cudaFree(S->d_err_pool);
     if (S->d_busy_ns) cudaFree(S->d_busy_ns);
     ctx_release(ctx);
     delete S;
@@ -871,8 +843,6 @@ extern "C" gd_status gd_server_get_stats(gd_server *S, gd_server_stats *out) {
   cudaSetDevice(S->ctx->device);
   GD_CUDA(cudaMemcpy(&ns, S->d_busy_ns, sizeof ns, cudaMemcpyDeviceToHost));
   out->cta_busy_s = (double)ns * 1e-9;
-  out->lane_run_s = S->lane_run_s.load();
-  out->lane_gap_s = S->lane_gap_s.load();
   out->host_launch_s = S->host_launch_s.load();
   return GD_OK;
 }
@@ -893,16 +863,14 @@ extern "C" gd_status gd_server_destroy(gd_server *S) {
   for (auto &kv : S->lanes) {
     Lane &L = *kv.second;
     cudaStreamSynchronize(L.stream);
-    if (L.d_items) cudaFree(L.d_items);
-    if (L.d_cta) cudaFree(L.d_cta);
-    if (L.d_groups) cudaFree(L.d_groups);
+    for (Lane::Desc &D : L.desc) {
+      if (D.items) cudaFreeHost(D.items);
+      if (D.cta) cudaFreeHost(D.cta);
+      if (D.groups) cudaFreeHost(D.groups);
+    }
     cudaEventDestroy(L.done);
-    cudaEventDestroy(L.t_start);
-    cudaEventDestroy(L.t_end);
-    cudaEventDestroy(L.t_end_prev);
     cudaStreamDestroy(L.stream);
   }
-  if (S->d_err_pool) cudaFree(S->d_err_pool);
   if (S->d_busy_ns) cudaFree(S->d_busy_ns);
   if (S->h_err_pool) cudaFreeHost(S->h_err_pool);
   ctx_release(S->ctx);

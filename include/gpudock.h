@@ -608,8 +608,6 @@ typedef struct gd_server_stats {
   double busy_s;            /* seconds the scheduler spent in iterations    */
   double cta_busy_s;        /* seconds the server's CTAs spent on SMs,      */
                             /* summed over CTAs (/ SMs / wall = occupancy)  */
-  double lane_run_s;        /* summed run time of the lanes' launches       */
-  double lane_gap_s;        /* summed GPU time between a lane's launches    */
   double host_launch_s;     /* scheduler-thread time spent issuing launches */
 } gd_server_stats;
 
