@@ -18,6 +18,7 @@ LIB = os.path.join(HERE, "_build", "libgdoracle.so")
 LIB_NATIVE = os.path.join(HERE, "_build", "libgdoracle_native.so")
 
 _libs = {}
+_max_threads = {}
 
 
 def reference_root():
@@ -77,6 +78,9 @@ def load(native: bool = False):
     lib.orc_bayes_total.argtypes = [P]
     lib.orc_bayes_total.restype = C.c_float
     _libs[key] = lib
+    # OpenMP's thread count is process-wide and a call with n_threads sets
+    # it for good: note the host's before any call does
+    _max_threads.setdefault("n", int(lib.orc_max_threads()))
     return lib
 
 
@@ -130,7 +134,7 @@ def energy_poses(cx: abi.Complex, poses: np.ndarray, prt_conf: int = 0, lig_conf
     raw = np.zeros((n, abi.NRAW), np.float64)
     asum = np.zeros((n, 5), np.float64)
     lib.orc_energy_poses(C.byref(cx.struct()), prt_conf, lig_conf, n, _p(poses), _p(terms),
-                         _p(raw), _p(asum), n_threads)
+                         _p(raw), _p(asum), n_threads or max_threads(native))
     return terms, raw, asum
 
 
@@ -150,7 +154,8 @@ def remc_run(cx: abi.Complex, steps_total: int, steps_per_exchange: int, minus_b
     params, mb = abi.mc_params(steps_total, steps_per_exchange, minus_beta, **kw)
     n_rep = cx.n_prt * cx.n_lig * len(mb)
     buf = abi.McLogBuffers(n_rep, len(mb), steps_total, bool(params.flags & abi.MC_RECORD))
-    st = load().orc_remc_run(C.byref(cx.struct()), C.byref(params), C.byref(buf.log), n_threads)
+    st = load().orc_remc_run(C.byref(cx.struct()), C.byref(params), C.byref(buf.log),
+                             n_threads or max_threads())
     if st != 0:
         raise RuntimeError(f"orc_remc_run: status {st}")
     return buf
@@ -159,11 +164,14 @@ def remc_run(cx: abi.Complex, steps_total: int, steps_per_exchange: int, minus_b
 def mc_sample(cx: abi.Complex, params: abi.GdMcParams, r0: int, n_rep: int, n_steps: int,
               n_threads: int = 0, native: bool = False) -> int:
     return int(load(native).orc_mc_sample(C.byref(cx.struct()), C.byref(params), r0, n_rep,
-                                          n_steps, n_threads))
+                                          n_steps, n_threads or max_threads(native)))
 
 
 def max_threads(native: bool = False) -> int:
-    return int(load(native).orc_max_threads())
+    """Threads an all-cores call uses: OpenMP's default for this process,
+    noted when the oracle was first loaded."""
+    load(native)
+    return _max_threads["n"]
 
 
 def mcc(cx: abi.Complex, ref_prt: int, prt_conf: int, lig_conf: int, m) -> float:
