@@ -438,6 +438,8 @@ template <typename T>
 static gd_status upload(gd_dcomplex *d, const std::vector<T> &h, const T **out) {
   void *p = nullptr;
   const size_t n = std::max<size_t>(h.size(), 1) * sizeof(T);
+  if (injected_alloc_failure(d->ctx))
+    return fail(GD_ENOMEM, "cudaMallocAsync of %zu bytes: out of memory (injected)", n);
   GD_CUDA(cudaMallocAsync(&p, n, d->ctx->stream));
   d->allocs.push_back(p);
   d->bytes += n;
@@ -730,6 +732,7 @@ static gd_status complex_upload_common(gd_ctx *ctx, const gd_complex *cx,
 }
 
 extern "C" gd_status gd_complex_upload(gd_ctx *ctx, const gd_complex *cx, gd_dcomplex **out) {
+  NvtxRange nvtx("gd_complex_upload");
   return complex_upload_common(ctx, cx, nullptr, 0, 0, out);
 }
 
@@ -775,6 +778,7 @@ static gd_status poses_launch(gd_ctx *ctx, const gd_dcomplex *d, const Tile &til
 extern "C" gd_status gd_energy_poses_dev(gd_ctx *ctx, const gd_dcomplex *d, int prt_conf,
                                          int lig_conf, int n_pose, const float *poses,
                                          float *terms, double *raw) {
+  NvtxRange nvtx("gd_energy_poses_dev");
   if (!ctx || !d) return fail(GD_EINVAL, "gd_energy_poses_dev: NULL handle");
   if (n_pose < 0) return fail(GD_EINVAL, "n_pose=%d", n_pose);
   if (prt_conf < 0 || prt_conf >= d->T.n_prt)
@@ -873,6 +877,13 @@ extern "C" gd_status gd_ctx_set_wait_test(gd_ctx *c, unsigned wait_limit, int ne
   c->wait_limit = wait_limit;
   // no run reaches this many MC steps, so a wait for it can only run out
   c->wait_bias = never_release ? (1 << 30) : 0;
+  return GD_OK;
+}
+
+extern "C" gd_status gd_ctx_set_alloc_fail(gd_ctx *c, int nth) {
+  if (!c) return fail(GD_EINVAL, "ctx is NULL");
+  if (nth < 0) return fail(GD_EINVAL, "gd_ctx_set_alloc_fail: nth=%d", nth);
+  c->alloc_fail_in.store(nth);
   return GD_OK;
 }
 

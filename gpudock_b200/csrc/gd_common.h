@@ -11,6 +11,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "gd_internal.h"
 
@@ -34,6 +35,15 @@ gd_status fail(gd_status st, const char *fmt, ...);
   } while (0)
 
 constexpr float kPI = 3.1415926535f;  // size.h:86
+
+// NVTX range over a host call (shown by profilers that attach a tool; free
+// otherwise).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Launch shape of the energy kernel: A atom groups x P tile groups of warps,
 // NA ligand atoms per warp.
@@ -69,6 +79,8 @@ struct gd_ctx {
   int split_mode = 0;      // CTAs per unit of MC launches (0: split_for's rule)
   uint32_t wait_limit = 0; // polls of a dependency wait before it gives up (0: default)
   int wait_bias = 0;       // added to every dependency wait's target (test hook)
+  std::atomic<int> alloc_fail_in{0};  // > 0: that many device allocations from now,
+                                      // the last one fails (test hook)
   std::atomic<int> refs{1};
   // autotuned launch shapes keyed by (ligand-size bucket, protein tiles)
   std::mutex tile_mu;
@@ -106,6 +118,14 @@ gd_status kernel_error(int code);
 // gd_energy_poses_noalloc on c's device (current) and stores the array's
 // address in c->noalloc_scratch (gd_noalloc.cu).  Called by gd_ctx_create.
 gd_status noalloc_attach(gd_ctx *c);
+// Test hook of gd_ctx_set_alloc_fail: true (and the hook off again) when
+// this device allocation through c is the one set to fail.
+inline bool injected_alloc_failure(gd_ctx *c) {
+  int n = c->alloc_fail_in.load();
+  while (n > 0 && !c->alloc_fail_in.compare_exchange_weak(n, n - 1)) {
+  }
+  return n == 1;
+}
 // Ligand-size bucket: sizes are rounded up to a multiple of 8 atoms; launch
 // shapes are chosen (and autotuned) per bucket and cover its largest size.
 int lna_bucket(int lna);

@@ -109,6 +109,9 @@ struct Ens {
 template <typename T>
 gd_status dalloc(Ens &E, T **out, size_t n) {
   void *p = nullptr;
+  if (injected_alloc_failure(E.ctx))
+    return fail(GD_ENOMEM, "cudaMallocAsync of %zu bytes: out of memory (injected)",
+                std::max<size_t>(n, 1) * sizeof(T));
   GD_CUDA(cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), E.ctx->stream));
   E.allocs.push_back(p);
   GD_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), E.ctx->stream));
@@ -898,11 +901,13 @@ extern "C" gd_status gd_remc_destroy(gd_remc *r) {
 extern "C" int gd_remc_n_rep(const gd_remc *r) { return r ? r->e.n_rep_total : 0; }
 
 extern "C" gd_status gd_remc_init(gd_remc *r) {
+  NvtxRange nvtx("gd_remc_init");
   if (!r) return fail(GD_EINVAL, "remc NULL");
   return ens_init(r->e);
 }
 
 extern "C" gd_status gd_remc_run(gd_remc *r, int n_steps) {
+  NvtxRange nvtx("gd_remc_run");
   if (!r) return fail(GD_EINVAL, "remc NULL");
   return ens_run(r->e, n_steps);
 }
@@ -941,6 +946,7 @@ extern "C" gd_status gd_remc_kernel_times(gd_remc *r, double *mc_ms, int *mc_lau
 }
 
 extern "C" gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc, gd_mc_log *log) {
+  NvtxRange nvtx("gd_run");
   const auto t0 = std::chrono::steady_clock::now();
   GD_TRY(validate_mc(mc));
   // one context per calling thread, kept between calls (its stream, side
@@ -1001,11 +1007,13 @@ extern "C" int gd_batch_n_launch_shapes(const gd_batch *b) {
 }
 
 extern "C" gd_status gd_batch_init(gd_batch *b) {
+  NvtxRange nvtx("gd_batch_init");
   if (!b) return fail(GD_EINVAL, "batch NULL");
   return ens_init(b->e);
 }
 
 extern "C" gd_status gd_batch_run(gd_batch *b, int n_steps) {
+  NvtxRange nvtx("gd_batch_run");
   if (!b) return fail(GD_EINVAL, "batch NULL");
   return ens_run(b->e, n_steps);
 }

@@ -196,11 +196,10 @@ __device__ __forceinline__ void make_rot(float a3, float a4, float a5, float *R)
 
 // Per-atom hydrophobic sums in shared memory: for tile group g, the float2
 // of atom pair h (slots ag + 2hA, ag + (2h+1)A) of atom group ag and lane
-// `lane` sits at float2 index ((g A + ag) NH + h) 32 + lane.  Index of the
-// float of slot a:
-__device__ __forceinline__ int hpc_at(int g, int a, int lane, int A, int NH) {
-  const int ag = a % A, k = a / A;
-  return ((((g * A + ag) * NH + (k >> 1)) * 32 + lane) << 1) + (k & 1);
+// `lane` sits at float2 index ((g A + ag) NH + h) 32 + lane (a warp reads
+// a pair's sums as one conflict-free 64-bit access).
+__device__ __forceinline__ int hpc_pair_at(int g, int ag, int h, int lane, int A, int NH) {
+  return ((g * A + ag) * NH + h) * 32 + lane;
 }
 
 // Warp 0 after the step's partial sums: cross-warp reduction in a fixed
@@ -227,14 +226,26 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
       for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
     }
     // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149), by
-    // slot (slot a holds one atom, s_lt its type)
-    for (int a = 0; a < lna; ++a) {
-      float h = 0.f;
-      for (int g = 0; g < P; ++g) h += s_hpc[hpc_at(g, a, lane, A, NH)];
-      const int lt = s_lt[a];
-      const float hh = __fdiv_rn(__fsub_rn(h, T.hpl0[lt]), T.hpl1[lt]);
-      S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
-    }
+    // slot (slot a = ag + A k holds one atom, s_lt its type), an atom pair's
+    // two slots at a time
+    const float2 *s_hpc2 = reinterpret_cast<const float2 *>(s_hpc);
+    for (int ag = 0; ag < A; ++ag)
+      for (int hp = 0; hp < NH; ++hp) {
+        if (ag + 2 * hp * A >= lna) break;
+        float2 v = make_float2(0.f, 0.f);
+        for (int g = 0; g < P; ++g) {
+          const float2 x = s_hpc2[hpc_pair_at(g, ag, hp, lane, A, NH)];
+          v.x += x.x;
+          v.y += x.y;
+        }
+        for (int j = 0; j < 2; ++j) {
+          const int a = ag + A * (2 * hp + j);
+          if (a >= lna) break;
+          const int lt = s_lt[a];
+          const float hh = __fdiv_rn(__fsub_rn(j ? v.y : v.x, T.hpl0[lt]), T.hpl1[lt]);
+          S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
+        }
+      }
     const double n = (double)lna;
     double raw[GD_NRAW];
     raw[0] = S[0] / n;
@@ -495,8 +506,7 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
   const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
   const bool hflag = (meta & META_HPC_BIT) != 0u;
   const uint32_t res = meta >> META_SEQ_SHIFT;
-  const bool psp_on = is_c2 && ((__ldg(&T.psp_mask[res >> 5]) >> (res & 31)) & 1u) != 0u;
-  const bool pm_on = psp_on || mcc_on;  // the d <= pmf0 block below
+  const bool pm_on = is_c2 || mcc_on;  // the d <= pmf0 block below
   // the largest squared distance at which a term below can fire for this
   // point: atom pairs that no lane has within it are skipped (warp-uniform)
   const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f, pm_on ? T.near_mcc2 : 0.0f));
@@ -538,7 +548,8 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
         const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
         const float dm = d + ((k & 1) ? T1.y : T1.x);
         if (dm <= 0.0f) {
-          if (psp_on) fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + res]);
+          if (is_c2 && ((__ldg(&T.psp_mask[res >> 5]) >> (res & 31)) & 1u))
+            fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + res]);
           if (mcc_on) {
             const int a = s_atom[ag + A * k];
             my_red[8 * 32] += 1.0;
@@ -1029,10 +1040,16 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
           for (int w = 0; w < W; ++w) acc += s_red[((size_t)w * NRED + i) * 32 + lane];
           xs[i * 32 + lane] = acc;
         }
-        for (int a = 0; a < lna; ++a) {
-          float h = 0.f;
-          for (int g = 0; g < P; ++g) h += s_hpc[hpc_at(g, a, lane, A, NH)];
-          xh[a * 32 + lane] = h;
+        const float2 *s_hpc2 = reinterpret_cast<const float2 *>(s_hpc);
+        float2 *xh2 = reinterpret_cast<float2 *>(xh);
+        for (int i = 0; i < A * NH; ++i) {  // atom pairs (ag, h) = (i / NH, i % NH)
+          float2 v = make_float2(0.f, 0.f);
+          for (int g = 0; g < P; ++g) {
+            const float2 x = s_hpc2[hpc_pair_at(g, i / NH, i % NH, lane, A, NH)];
+            v.x += x.x;
+            v.y += x.y;
+          }
+          xh2[i * 32 + lane] = v;
         }
       }
       cluster_sync_all();
@@ -1042,10 +1059,16 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
           for (int r = 0; r < csize; ++r) acc += cluster_map(xs, r)[i * 32 + lane];
           s_red[(size_t)i * 32 + lane] = acc;  // warp 0's slots
         }
-        for (int a = 0; a < lna; ++a) {
-          float h = 0.f;
-          for (int r = 0; r < csize; ++r) h += cluster_map(xh, r)[a * 32 + lane];
-          s_hpc[hpc_at(0, a, lane, A, NH)] = h;  // tile group 0's slots
+        float2 *s_hpc2 = reinterpret_cast<float2 *>(s_hpc);
+        const float2 *xh2 = reinterpret_cast<const float2 *>(xh);
+        for (int i = 0; i < A * NH; ++i) {
+          float2 v = make_float2(0.f, 0.f);
+          for (int r = 0; r < csize; ++r) {
+            const float2 x = cluster_map(xh2, r)[i * 32 + lane];
+            v.x += x.x;
+            v.y += x.y;
+          }
+          s_hpc2[hpc_pair_at(0, i / NH, i % NH, lane, A, NH)] = v;  // tile group 0's
         }
         finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, A, NH, lane, rep, active, prt_conf,
                           lig_conf, step, crank0 == 0);

@@ -246,6 +246,7 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
 // Uploads the request's tables, allocates its state on its lane's stream and
 // fills its KItem.
 gd_status admit(gd_server *S, Req *r) {
+  NvtxRange nvtx("gd_server admit");
   SrvProtein &P = *S->proteins[r->protein];
   GD_TRY(gd_complex_upload_shared(S->ctx, &r->cx, P.dcx, 0, P.prt.n_conf, &r->dcx));
   Lane *L = nullptr;
@@ -254,6 +255,8 @@ gd_status admit(gd_server *S, Req *r) {
   r->stream = L->stream;
   cudaStream_t s = L->stream;
   const size_t n = (size_t)r->n_rep;
+  if (injected_alloc_failure(S->ctx))
+    return fail(GD_ENOMEM, "request state: out of memory (injected)");
   GD_CUDA(cudaMallocAsync(&r->d_m_old, n * 6 * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_e_old, n * GD_NTERM * sizeof(float), s));
   GD_CUDA(cudaMallocAsync(&r->d_cmcc, n * sizeof(float), s));
@@ -304,6 +307,7 @@ gd_status admit(gd_server *S, Req *r) {
 // at its own step, for its own step count), plus the exchange kernel for
 // groups that do not fit a CTA.  Asynchronous on the lane's stream.
 gd_status launch_lane(gd_server *S, Lane &L, const std::vector<Req *> &rs, int mode) {
+  NvtxRange nvtx(mode == KMODE_INIT ? "gd_server lane init" : "gd_server lane launch");
   if (rs.empty()) return GD_OK;
   cudaStream_t s = L.stream;
   std::vector<KItem> items;

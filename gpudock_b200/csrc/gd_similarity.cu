@@ -324,6 +324,7 @@ static gd_status similarity_run(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
 
 extern "C" gd_status gd_similarity_matrix(gd_ctx *ctx, const gd_dcomplex *d, int n_conf,
                                           const float *confs, float *similarity) {
+  NvtxRange nvtx("gd_similarity_matrix");
   if (n_conf > 0 && !similarity) return fail(GD_EINVAL, "similarity NULL");
   return similarity_run(ctx, d, n_conf, confs, nullptr, similarity);
 }

@@ -49,6 +49,7 @@ def _declare(lib):
         "gd_ctx_set_schedule": ([P, i32, i32], i32),
         "gd_ctx_set_split": ([P, i32], i32),
         "gd_ctx_set_wait_test": ([P, C.c_uint, i32], i32),
+        "gd_ctx_set_alloc_fail": ([P, i32], i32),
         "gd_remc_snapshot": ([P, P, C.c_size_t, C.POINTER(C.c_size_t)], i32),
         "gd_remc_restore": ([P, P, C.c_size_t], i32),
         "gd_batch_snapshot": ([P, P, C.c_size_t, C.POINTER(C.c_size_t)], i32),
@@ -202,6 +203,11 @@ class Context:
         (gd_ctx_set_wait_test).  set_wait_test(0, False) restores the default."""
         check(self._lib.gd_ctx_set_wait_test(self.h, int(wait_limit), int(never_release)),
               "gd_ctx_set_wait_test")
+
+    def set_alloc_fail(self, nth: int):
+        """Test hook: the nth device allocation from now fails with GD_ENOMEM
+        (gd_ctx_set_alloc_fail); 0 turns it off."""
+        check(self._lib.gd_ctx_set_alloc_fail(self.h, int(nth)), "gd_ctx_set_alloc_fail")
 
     def close(self):
         if self.h:
@@ -510,6 +516,11 @@ class Server:
 
     def cancel(self, rid: int):
         check(self._lib.gd_server_cancel(self.h, C.c_uint64(rid)), "gd_server_cancel")
+
+    def set_alloc_fail(self, nth: int):
+        """Test hook on the server's context (gd_ctx_set_alloc_fail)."""
+        check(self._lib.gd_ctx_set_alloc_fail(self._lib.gd_server_context(self.h), int(nth)),
+              "gd_ctx_set_alloc_fail")
 
     def set_split(self, split: int):
         """CTAs per request unit for requests admitted from now on (0: the

@@ -668,6 +668,12 @@ gd_status gd_fma_peak(gd_ctx *ctx, int n_blocks, int iters, float *ms,
  * restores the defaults (runs created meanwhile keep the setting their
  * captured launches were built with). */
 gd_status gd_ctx_set_wait_test(gd_ctx *ctx, unsigned wait_limit, int never_release);
+/* Test hook for allocation failures: the nth device allocation the library
+ * makes through ctx from now on (uploads, run state, server requests; nth
+ * >= 1) fails as cudaMallocAsync does on a full device, and the call that
+ * made it returns GD_ENOMEM after freeing what it had allocated.  The hook
+ * is then off again; nth = 0 turns it off. */
+gd_status gd_ctx_set_alloc_fail(gd_ctx *ctx, int nth);
 /* The persistent schedule (host only, no device): n_units units of cost[u]
  * per MC step and steps[u] steps over `machines` CTAs.  pieces[4 k ..] =
  * {unit, first step, end step, wait} for k < piece_off[*n_used], CTA m's in

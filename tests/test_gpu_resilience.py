@@ -9,7 +9,11 @@
    traps or hangs: the waits end by their limit.
 2. A run snapshotted at step 50 and restored into a new handle continues
    bit for bit as the same run without the break (the reference keeps no
-   random state in its dumps, util_d.cu:85-92, and cannot resume)."""
+   random state in its dumps, util_d.cu:85-92, and cannot resume).
+3. Device allocations that fail (injected with gd_ctx_set_alloc_fail) give
+   GD_ENOMEM, free what the failing call had allocated, and leave the
+   context and the server usable (the reference exits on any CUDA error,
+   include_cuda/cutil_yeah.h:26-47)."""
 import numpy as np
 import pytest
 
@@ -172,3 +176,56 @@ def test_batch_snapshot_restore():
         d.close()
     base.close()
     ctx.close()
+
+
+def _pool_used():
+    from cuda.bindings import runtime as rt
+    assert rt.cudaDeviceSynchronize()[0] == rt.cudaError_t.cudaSuccess
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(used)
+
+
+def test_injected_allocation_failures():
+    """A device allocation that fails (injected at the library's allocation
+    sites, as cudaMallocAsync fails on a full device) makes the call return
+    GD_ENOMEM, frees what the call had allocated, and leaves the context,
+    and the server, working."""
+    ctx = lib.Context(0)
+    cx, n_tmp = _complex("fused")
+    _, mb = lib.set_temperature(n_tmp, 0.004, 0.04)
+    used0 = _pool_used()
+    for nth in (1, 3, 7):  # upload: the protein, the tables, the ligand ...
+        ctx.set_alloc_fail(nth)
+        with pytest.raises(lib.GdError) as exc:
+            lib.DeviceComplex(ctx, cx)
+        assert exc.value.status == abi.GD_ENOMEM and "injected" in str(exc.value)
+        assert _pool_used() == used0
+    d = lib.DeviceComplex(ctx, cx)  # the hook is off again
+    used1 = _pool_used()
+    ctx.set_alloc_fail(2)  # the run's state
+    with pytest.raises(lib.GdError) as exc:
+        lib.Remc(d, 20, 10, mb, seed=3)
+    assert exc.value.status == abi.GD_ENOMEM
+    assert _pool_used() == used1
+    r = lib.Remc(d, 20, 10, mb, seed=3)
+    r.init()
+    r.run(20)
+    out = r.read()
+    assert np.isfinite(out.energy).all()
+    r.close()
+    d.close()
+    ctx.close()
+    # a served request whose admission fails, between two that succeed
+    srv = lib.Server(0, hbm_budget_bytes=1 << 30, max_active=4, steps_per_launch=10)
+    pid = srv.add_protein(cx)
+    ok0 = srv.wait(srv.submit(pid, cx, 20, 10, mb, n_prt=cx.n_prt, seed=4))
+    srv.set_alloc_fail(1)
+    bad = srv.submit(pid, cx, 20, 10, mb, n_prt=cx.n_prt, seed=4)
+    with pytest.raises(lib.GdError) as exc:
+        srv.wait(bad)
+    assert exc.value.status == abi.GD_ENOMEM
+    ok1 = srv.wait(srv.submit(pid, cx, 20, 10, mb, n_prt=cx.n_prt, seed=4))
+    assert np.array_equal(ok0.energy, ok1.energy)
+    srv.close()
