@@ -822,6 +822,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       32 - __clz(__reduce_or_sync(0xffffffffu, lane < PT_ROWS ? my_hmask[lane] : 0u));
   // the host's bound must cover this warp; report it if not (code 3)
   if (my_nhb > HB && lane == 0) atomicExch(R.err, 3);
+  // warps whose atoms need fewer H-bond pairs than the launch's HB take a
+  // variant with one pair less (most warps of a ligand: the capable atoms
+  // come first in the slot order, dealt round robin over the atom groups)
+  constexpr int kHB1 = HB > 1 ? HB - 1 : HB;
 
   for (int si = 0; si < n_steps; ++si) {
     const int step = step_base + si;
@@ -932,12 +936,16 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         float thr_l = T.near4[((meta_l & META_HPC_BIT) ? 1 : 0) |
                               ((((meta_l >> META_CLASS_SHIFT) & 3u) == 2u) ? 2 : 0)];
         if (mcc_on) thr_l = fmaxf(thr_l, T.near_mcc2);
-        // two variants per kernel (each is a long unrolled body: more of them
-        // cost more in instruction fetch than skipping H-bond work saves)
+        // three variants per kernel: no H-bond term, HB - 1 pairs (warps that
+        // need no more) and HB pairs; each is a long unrolled body, so more
+        // of them would cost more in instruction fetch than they save
         const uint32_t close =
             (chunk_hdb && my_nhb > 0)
-                ? chunk_fast<NH, HB>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K, thr_l,
-                                     fvdw, fpmf, fhdb, fek)
+                ? (my_nhb <= kHB1
+                       ? chunk_fast<NH, kHB1>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
+                                              thr_l, fvdw, fpmf, fhdb, fek)
+                       : chunk_fast<NH, HB>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K,
+                                            thr_l, fvdw, fpmf, fhdb, fek))
                 : chunk_fast<NH, 0>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K, thr_l,
                                     fvdw, fpmf, fhdb, fek);
         for (uint32_t m = close; m != 0u; m &= m - 1u) {
