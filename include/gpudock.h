@@ -562,8 +562,10 @@ gd_status gd_run(const gd_complex *cx, const gd_mc_params *mc,
 /* share steps_per_exchange; each keeps its own replicas, temperatures,     */
 /* random stream and counters.  Complexes with the same launch shape share  */
 /* one launch; with whole exchange groups per CTA (32 % n_tmp == 0) the     */
-/* exchange runs inside the kernel and a run is one launch per shape,       */
-/* otherwise the interval sequence is replayed from a captured CUDA graph.  */
+/* exchange runs inside the kernel and a run is one launch per shape (side  */
+/* by side), replayed from one captured CUDA graph once a run length is     */
+/* used again; otherwise the interval sequence is replayed from a captured  */
+/* CUDA graph.                                                              */
 /* ------------------------------------------------------------------------ */
 typedef struct gd_batch gd_batch;
 
