@@ -117,8 +117,14 @@ struct Lane {
   } desc[2];
 };
 
-using LaneKey = std::tuple<int, int, int, int, int, int, int, int>;
-constexpr int kMaxLanes = 256;
+// (A, P, NA, stages, resident, group-major, steps per exchange, split, sub-lane)
+using LaneKey = std::tuple<int, int, int, int, int, int, int, int, int>;
+constexpr int kMaxLanes = 512;
+// Lanes per launch shape.  A lane relaunches only when the slowest CTA of its
+// launch has finished, so its other SMs wait meanwhile unless other lanes'
+// CTAs are queued; requests of one shape dealt over several lanes (each
+// with its own stream) keep more CTAs queued.
+constexpr int kSubLanes = 4;
 
 }  // namespace
 
@@ -220,12 +226,23 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   pick_stages(T, t, &ns, &res, split);
   const bool gm = (32 % r->mc.n_tmp) == 0;
   const int spe = r->mc.steps_per_exchange;
-  const LaneKey key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe, split};
-  auto it = S->lanes.find(key);
-  if (it != S->lanes.end()) {
-    *out = it->second.get();
+  // the shape's least loaded lane; a new one while that lane holds requests
+  // and the shape has fewer than kSubLanes
+  Lane *best = nullptr;
+  int n_sub = 0;
+  for (int sub = 0; sub < kSubLanes; ++sub) {
+    auto it = S->lanes.find(LaneKey{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe, split, sub});
+    if (it == S->lanes.end()) break;
+    ++n_sub;
+    Lane *L = it->second.get();
+    if (!best || L->members.size() + L->fresh.size() < best->members.size() + best->fresh.size())
+      best = L;
+  }
+  if (best && ((best->members.empty() && best->fresh.empty()) || n_sub == kSubLanes)) {
+    *out = best;
     return GD_OK;
   }
+  const LaneKey key{t.A, t.P, t.NA, ns, res, gm ? 1 : 0, spe, split, n_sub};
   auto L = std::make_unique<Lane>();
   L->tile = t;
   L->ns = ns;
@@ -234,7 +251,7 @@ gd_status lane_for(gd_server *S, const Req *r, Lane **out) {
   L->spe = spe;
   L->split = split;
   const int slot = (int)S->lanes.size();
-  if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d launch shapes in the server", kMaxLanes);
+  if (slot >= kMaxLanes) return fail(GD_ENOMEM, "more than %d lanes in the server", kMaxLanes);
   GD_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
   GD_CUDA(cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming));
   L->h_err = S->h_err_pool + slot;
