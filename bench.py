@@ -495,7 +495,7 @@ def form_poses(ctx, stream, seed, n_pose=1 << 20):
     proteins of 2,000 / 4,000 / 8,000 / 16,000 points (pose-energies/s)."""
     import dataclasses
     import torch
-    from gpudock_b200 import lib, synth
+    from gpudock_b200 import abi, lib, synth
     w = synth.WORKLOADS["poses_48"]
     rng = np.random.default_rng(seed + 3)
     poses_h = synth.random_poses(rng, n_pose, box=w.extra["box"])
@@ -505,13 +505,22 @@ def form_poses(ctx, stream, seed, n_pose=1 << 20):
     for pnp in w.extra["pnp_sweep"]:
         cx = synth.make_complex(dataclasses.replace(w.spec, pnp=pnp), seed=seed + pnp)
         d = lib.DeviceComplex(ctx, cx)
-        tile, _ = d.autotune()
         run = lambda: d.energy_poses_dev(n_pose, poses.data_ptr(), terms.data_ptr())
+        # the other shapes that cover 48 atoms, timed on the sweep itself,
+        # beside the autotuner's choice (which is timed on MC steps)
+        alt = {}
+        for t in ((5, 2, 10), (6, 2, 8), (8, 1, 6), (12, 1, 4)):
+            lib.check(ctx._lib.gd_ctx_set_tile(ctx.h, cx.lna, pnp, abi.GdTile(*t)),
+                      "gd_ctx_set_tile")
+            run()
+            alt[",".join(map(str, t))] = _event_ms(stream, run)
+        tile, _ = d.autotune()
         run()
         ms = _event_ms(stream, run)
         out[str(pnp)] = {"value": n_pose / (ms * 1e-3), "unit": "pose-energies/s",
                          "fp32_tflops": FLOP_PER_PAIR * n_pose * cx.lna * pnp / (ms * 1e-3)
                          / 1e12, "tile": list(tile),
+                         "ms_by_tile_A_P_NA": alt,
                          "cpu_baseline": cpu_poses_rate(cx, poses_h)}
         d.close()
     return {"workload": w.name, "n_pose": n_pose, "by_protein_points": out}
