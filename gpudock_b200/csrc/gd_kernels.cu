@@ -492,24 +492,29 @@ __device__ __forceinline__ uint32_t chunk_fast(const float2 (&nx)[NH], const flo
 // are recomputed per atom pair; p is the point's index in the protein.
 // The hydrophobic polynomial runs packed over an atom pair, branch-free
 // (zero beyond 9 A and for padding slots), into the pair's float2 of
-// per-atom sums (my_hpc2 + 32 h).  The PSP table is read only for residues
-// where some atom type of this ligand has a nonzero entry (T.psp_mask): the
-// others would add exactly zero.
+// per-atom sums of the chunk (hacc[h], added to the shared-memory sums once
+// per chunk).  The contact test d <= pmf0 (a distance and a table read per
+// atom) runs only with the MCC score on or on residues where some atom type
+// of this ligand has a nonzero PSP entry (T.psp_mask): elsewhere the PSP
+// term adds exactly zero.
 template <int NA>
 __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const float2 (&ny)[NA / 2],
                                             const float2 (&nz)[NA / 2], const float4 &Ap,
                                             float hpp, uint32_t meta, const float4 *pp,
                                             const KTables &T, const float *s_q, const int *s_lt,
-                                            const int *s_atom, float2 *my_hpc2, int A, int ag,
+                                            const int *s_atom, float2 (&hacc)[NA / 2], int A, int ag,
                                             int n_my, float inv_el1, float &fnear, float &fpsp,
                                             bool mcc_on, int p, double *my_red) {
   const bool is_c2 = ((meta >> META_CLASS_SHIFT) & 3u) == 2u;
   const bool hflag = (meta & META_HPC_BIT) != 0u;
   const uint32_t res = meta >> META_SEQ_SHIFT;
-  const bool pm_on = is_c2 || mcc_on;  // the d <= pmf0 block below
+  // the d <= pmf0 block below: the contact count of the MCC score, or a PSP
+  // entry of this residue for some atom type of the ligand
+  const bool psp_on = is_c2 && ((__ldg(&T.psp_mask[res >> 5]) >> (res & 31)) & 1u) != 0u;
+  const bool thr_pm = is_c2 || mcc_on;  // the threshold stays the point kind's
   // the largest squared distance at which a term below can fire for this
   // point: atom pairs that no lane has within it are skipped (warp-uniform)
-  const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f, pm_on ? T.near_mcc2 : 0.0f));
+  const float thr = fmaxf(T.near_ele2, fmaxf(hflag ? 81.0f : 0.0f, thr_pm ? T.near_mcc2 : 0.0f));
   const float c1 = 3.5f / 81.0f;
   const float c2 = -4.5f / 81.0f / 81.0f;
   const float c3 = 2.5f / 81.0f / 81.0f / 81.0f;
@@ -527,7 +532,7 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
       float2 poly = fma2(make_float2(-q.x, -q.y), d2p, dup2(1.0f));
       poly.x = (d2p.x <= 81.0f && 2 * h < n_my) ? poly.x : 0.0f;
       poly.y = (d2p.y <= 81.0f && 2 * h + 1 < n_my) ? poly.y : 0.0f;
-      my_hpc2[h * 32] = fma2(dup2(hpp), poly, my_hpc2[h * 32]);
+      hacc[h] = fma2(dup2(hpp), poly, hacc[h]);
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -543,13 +548,12 @@ __device__ __forceinline__ void close_range(const float2 (&nx)[NA / 2], const fl
           fnear = fmaf(s_q[ag + A * k] * Ap.w, gnear - rk * inv_el1, fnear);
         }
       }
-      if (pm_on && k < n_my && d2 <= T.near_mcc2) {
+      if ((psp_on || mcc_on) && k < n_my && d2 <= T.near_mcc2) {
         const float d = d2 * frsqrt(d2);
         const float4 T1 = pp[(k >> 1) * 2 * PT_ROWS + 1];
         const float dm = d + ((k & 1) ? T1.y : T1.x);
         if (dm <= 0.0f) {
-          if (is_c2 && ((__ldg(&T.psp_mask[res >> 5]) >> (res & 31)) & 1u))
-            fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + res]);
+          if (psp_on) fpsp += __ldg(&T.psp[(size_t)s_lt[ag + A * k] * T.psp_ncol + res]);
           if (mcc_on) {
             const int a = s_atom[ag + A * k];
             my_red[8 * 32] += 1.0;
@@ -948,13 +952,22 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
                                             thr_l, fvdw, fpmf, fhdb, fek))
                 : chunk_fast<NH, 0>(nx, ny, nz, ta, tb, j0, j1, my_ptab, my_htab, K, thr_l,
                                     fvdw, fpmf, fhdb, fek);
-        for (uint32_t m = close; m != 0u; m &= m - 1u) {
-          const int j = j0 + __ffs(m) - 1;
-          const uint32_t meta = __float_as_uint(tb[j].y);
-          close_range<NA>(nx, ny, nz, ta[j], tb[j].x, meta,
-                          my_ptab + (int)(meta & META_TYPE_MASK) * 2, T, s_q, s_lt, s_atom,
-                          my_hpc2, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
-                          my_red);
+        if (close) {
+          // the chunk's hydrophobic sums in registers, added to the per-atom
+          // sums once per chunk
+          float2 hacc[NH];
+#pragma unroll
+          for (int h = 0; h < NH; ++h) hacc[h] = make_float2(0.f, 0.f);
+          for (uint32_t m = close; m != 0u; m &= m - 1u) {
+            const int j = j0 + __ffs(m) - 1;
+            const uint32_t meta = __float_as_uint(tb[j].y);
+            close_range<NA>(nx, ny, nz, ta[j], tb[j].x, meta,
+                            my_ptab + (int)(meta & META_TYPE_MASK) * 2, T, s_q, s_lt, s_atom,
+                            hacc, A, ag, n_my, inv_el1, fnear, fpsp, mcc_on, t * TILE_PTS + j,
+                            my_red);
+          }
+#pragma unroll
+          for (int h = 0; h < NH; ++h) my_hpc2[h * 32] = add2(my_hpc2[h * 32], hacc[h]);
         }
         float fele = 0.f;
 #pragma unroll
