@@ -3,9 +3,9 @@
 // dock_kernel: one CTA owns up to 32 replicas (or poses) of one complex that
 // share one protein conformation; lane i of every compute warp is replica i,
 // so protein-point and type-table reads are warp-uniform shared-memory
-// broadcasts.  The compute warps form an A x P grid: warp (ag, pg) keeps NA
-// ligand atoms a = ag + A k in registers and sweeps the protein tiles
-// t = pg, pg + P, ...  The protein conformation is staged in shared memory in
+// broadcasts.  The compute warps form an A x P grid: warp (ag, pg) (warp
+// number pg + P ag) keeps NA ligand atoms a = ag + A k in registers and
+// sweeps the protein tiles t = pg, pg + P, ...  The protein conformation is staged in shared memory in
 // 128-point tiles by the TMA engine (cp.async.bulk + mbarrier), once per
 // launch when it fits (resident) or through an 8-stage ring that the last
 // warp to finish a stage refills (then P = 1).  Per step every warp writes
@@ -202,8 +202,35 @@ __device__ __forceinline__ int hpc_pair_at(int g, int ag, int h, int lane, int A
   return ((g * A + ag) * NH + h) * 32 + lane;
 }
 
+// Hydrophobic restraint (calcenergy_d.cu:143-149) of atom pair hp of atom
+// group ag: the P tile groups' sums of the pair's two slots added in group
+// order, then 0.5 hh^2 - hpl2 with hh = (sum - hpl0) / hpl1 for each slot
+// that holds an atom (0 for a slot past the ligand).
+__device__ __forceinline__ float2 hpc_restraint(const KTables &T, const float2 *s_hpc2,
+                                                const int *s_lt, int P, int A, int NH, int ag,
+                                                int hp, int lane) {
+  float2 v = make_float2(0.f, 0.f);
+  for (int g = 0; g < P; ++g) {
+    const float2 x = s_hpc2[hpc_pair_at(g, ag, hp, lane, A, NH)];
+    v.x += x.x;
+    v.y += x.y;
+  }
+  float r[2] = {0.f, 0.f};
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int a = ag + A * (2 * hp + j);
+    if (a < T.lna) {
+      const int lt = s_lt[a];
+      const float hh = __fdiv_rn(__fsub_rn(j ? v.y : v.x, T.hpl0[lt]), T.hpl1[lt]);
+      r[j] = __fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
+    }
+  }
+  return make_float2(r[0], r[1]);
+}
+
 // Warp 0 after the step's partial sums: cross-warp reduction in a fixed
-// order, hydrophobic transform per atom, normalisation and total in the
+// order, hydrophobic restraint per atom (hpc_done: already transformed by the
+// warps into tile group 0's slots), normalisation and total in the
 // reference's order, then the pose output, or the Metropolis decision (with
 // the trajectory record) and, at the end of an interval, the in-CTA
 // temperature exchange.  Kept out of line so its registers do not burden the
@@ -213,7 +240,7 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
                                          double *s_red, const float *s_hpc, const int *s_lt,
                                          int W, int P, int A, int NH, int lane, int rep,
                                          bool active, int prt_conf, int lig_conf, int step,
-                                         bool primary) {
+                                         bool primary, bool hpc_done) {
   const KTables &T = I.T;
   const int lna = T.lna;
   const float lcx = T.lig_center[0], lcy = T.lig_center[1], lcz = T.lig_center[2];
@@ -225,26 +252,17 @@ __device__ __noinline__ void finish_step(const KRun &R, const KItem &I, LaneStat
 #pragma unroll
       for (int i = 0; i < NRED; ++i) S[i] += red[i * 32 + lane];
     }
-    // hydrophobic restraint per ligand atom (calcenergy_d.cu:143-149), by
-    // slot (slot a = ag + A k holds one atom, s_lt its type), an atom pair's
-    // two slots at a time
+    // hydrophobic restraint per ligand atom, by slot (slot a = ag + A k holds
+    // one atom, s_lt its type), an atom pair's two slots at a time, in slot
+    // order
     const float2 *s_hpc2 = reinterpret_cast<const float2 *>(s_hpc);
     for (int ag = 0; ag < A; ++ag)
       for (int hp = 0; hp < NH; ++hp) {
         if (ag + 2 * hp * A >= lna) break;
-        float2 v = make_float2(0.f, 0.f);
-        for (int g = 0; g < P; ++g) {
-          const float2 x = s_hpc2[hpc_pair_at(g, ag, hp, lane, A, NH)];
-          v.x += x.x;
-          v.y += x.y;
-        }
-        for (int j = 0; j < 2; ++j) {
-          const int a = ag + A * (2 * hp + j);
-          if (a >= lna) break;
-          const int lt = s_lt[a];
-          const float hh = __fdiv_rn(__fsub_rn(j ? v.y : v.x, T.hpl0[lt]), T.hpl1[lt]);
-          S[5] += (double)__fsub_rn(__fmul_rn(__fmul_rn(0.5f, hh), hh), T.hpl2[lt]);
-        }
+        const float2 r = hpc_done ? s_hpc2[hpc_pair_at(0, ag, hp, lane, A, NH)]
+                                  : hpc_restraint(T, s_hpc2, s_lt, P, A, NH, ag, hp, lane);
+        S[5] += (double)r.x;
+        if (ag + A * (2 * hp + 1) < lna) S[5] += (double)r.y;
       }
     const double n = (double)lna;
     double raw[GD_NRAW];
@@ -775,7 +793,13 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   }
 
   // ---- compute warps -----------------------------------------------------
-  const int ag = warp % A, pg = warp / A;
+  // warp w = pg + P ag: an atom group's P warps sit on P different schedulers
+  // (w mod 4), so the groups whose atoms carry more H-bond pairs (the first
+  // ones: capable atoms are dealt round robin from group 0) do not pile onto
+  // one scheduler.  lw = pg A + ag numbers the warp's reduction slots and LHM
+  // records, which keeps the order of every sum.
+  const int ag = warp / P, pg = warp % P;
+  const int lw = pg * A + ag;
   const int lna = T.lna;
   const bool active = lane < n_act;
   const int rep = lane_rep;                    // local replica / pose index
@@ -900,7 +924,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     // ---- pair terms over the protein tiles -----------------------------------
     // FP64 sums of this lane live in the warp's own reduction slots (read by
     // warp 0 after the barrier), which keeps registers for the pair loop
-    double *my_red = s_red + (size_t)warp * NRED * 32 + lane;
+    double *my_red = s_red + (size_t)lw * NRED * 32 + lane;
 #pragma unroll
     for (int i = 0; i < NRED; ++i) my_red[i * 32] = 0.0;
     // resident: the tile groups take the 32-point chunks round robin
@@ -1022,8 +1046,8 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         }
       }
     }
-    // ---- LHM position restraints: MCS records m = warp, warp + W, ... -------
-    for (int m = crank0 == 0 ? warp : T.pos; m < T.pos; m += W) {
+    // ---- LHM position restraints: MCS records m = lw, lw + W, ... -----------
+    for (int m = crank0 == 0 ? lw : T.pos; m < T.pos; m += W) {
       float sv = 0.f;
       const float4 *Mm = T.mcs + (size_t)m * lna;
       for (int l = 0; l < lna; ++l) {
@@ -1092,11 +1116,23 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
           s_hpc2[hpc_pair_at(0, i / NH, i % NH, lane, A, NH)] = v;  // tile group 0's
         }
         finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, A, NH, lane, rep, active, prt_conf,
-                          lig_conf, step, crank0 == 0);
+                          lig_conf, step, crank0 == 0, false);
       }
-    } else if (warp == 0) {
-      finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, A, NH, lane, rep, active, prt_conf,
-                        lig_conf, step, true);
+    } else {
+      // the hydrophobic restraints, spread over the warps (atom pairs
+      // i = lw, lw + W, ... of the A x NH), each left in tile group 0's slot
+      // of its pair; warp 0 adds them up in slot order
+      float2 *s_hpc2 = reinterpret_cast<float2 *>(s_hpc);
+      for (int i = lw; i < A * NH; i += W) {
+        const int ai = i / NH, hp = i % NH;
+        if (ai + 2 * hp * A >= lna) continue;
+        const float2 r = hpc_restraint(T, s_hpc2, s_lt, P, A, NH, ai, hp, lane);
+        s_hpc2[hpc_pair_at(0, ai, hp, lane, A, NH)] = r;
+      }
+      named_sync(1, W * 32);
+      if (warp == 0)
+        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, A, NH, lane, rep, active, prt_conf,
+                          lig_conf, step, true, true);
     }
     // the next step's first barrier orders warp 0's updates (and its use of
     // s_red for the exchange) before any other warp touches them again
