@@ -1119,19 +1119,26 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
                           lig_conf, step, crank0 == 0, false);
       }
     } else {
-      // the hydrophobic restraints, spread over the warps (atom pairs
-      // i = lw, lw + W, ... of the A x NH), each left in tile group 0's slot
-      // of its pair; warp 0 adds them up in slot order
+      // spread over the warps (tasks i = lw, lw + W, ...): the cross-warp sum
+      // of each of the NRED terms (in warp-slot order, into slot 0) and the
+      // hydrophobic restraint of each of the A x NH atom pairs (into tile
+      // group 0's slot of the pair); warp 0 then finishes from slot 0 alone
       float2 *s_hpc2 = reinterpret_cast<float2 *>(s_hpc);
-      for (int i = lw; i < A * NH; i += W) {
-        const int ai = i / NH, hp = i % NH;
-        if (ai + 2 * hp * A >= lna) continue;
-        const float2 r = hpc_restraint(T, s_hpc2, s_lt, P, A, NH, ai, hp, lane);
-        s_hpc2[hpc_pair_at(0, ai, hp, lane, A, NH)] = r;
+      for (int i = lw; i < NRED + A * NH; i += W) {
+        if (i < NRED) {
+          double acc = 0.0;
+          for (int w = 0; w < W; ++w) acc += s_red[((size_t)w * NRED + i) * 32 + lane];
+          s_red[(size_t)i * 32 + lane] = acc;
+        } else {
+          const int ai = (i - NRED) / NH, hp = (i - NRED) % NH;
+          if (ai + 2 * hp * A >= lna) continue;
+          const float2 r = hpc_restraint(T, s_hpc2, s_lt, P, A, NH, ai, hp, lane);
+          s_hpc2[hpc_pair_at(0, ai, hp, lane, A, NH)] = r;
+        }
       }
       named_sync(1, W * 32);
       if (warp == 0)
-        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, W, P, A, NH, lane, rep, active, prt_conf,
+        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, P, A, NH, lane, rep, active, prt_conf,
                           lig_conf, step, true, true);
     }
     // the next step's first barrier orders warp 0's updates (and its use of
