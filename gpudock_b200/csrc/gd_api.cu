@@ -862,6 +862,13 @@ extern "C" gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines) {
   return GD_OK;
 }
 
+extern "C" gd_status gd_ctx_set_schedule_tail(gd_ctx *ctx, int tail) {
+  if (!ctx) return fail(GD_EINVAL, "gd_ctx_set_schedule_tail: NULL context");
+  if (tail < 0 || tail > 64) return fail(GD_EINVAL, "gd_ctx_set_schedule_tail: tail=%d", tail);
+  ctx->sched_tail = tail;
+  return GD_OK;
+}
+
 extern "C" gd_status gd_ctx_set_split(gd_ctx *ctx, int split) {
   if (!ctx) return fail(GD_EINVAL, "gd_ctx_set_split: NULL context");
   if (split < 0 || split > 8 || (split & (split - 1)))
@@ -884,6 +891,34 @@ extern "C" gd_status gd_ctx_set_alloc_fail(gd_ctx *c, int nth) {
   if (!c) return fail(GD_EINVAL, "ctx is NULL");
   if (nth < 0) return fail(GD_EINVAL, "gd_ctx_set_alloc_fail: nth=%d", nth);
   c->alloc_fail_in.store(nth);
+  return GD_OK;
+}
+
+extern "C" gd_status gd_schedule_queue(const double *cost, const int *steps, int n_units,
+                                       int machines, int tail, int *pieces, int cap,
+                                       int *piece_off, int *n_queue) {
+  if (n_units < 0 || machines < 1 || tail < 0 || cap < 0 || !piece_off || !n_queue ||
+      (n_units > 0 && (!cost || !steps || !pieces)))
+    return fail(GD_EINVAL, "gd_schedule_queue: bad arguments");
+  std::vector<double> c(cost, cost + n_units);
+  std::vector<int> s(steps, steps + n_units);
+  for (int u = 0; u < n_units; ++u)
+    if (!(c[u] > 0.0) || s[u] < 0)
+      return fail(GD_EINVAL, "gd_schedule_queue: unit %d has cost %g, %d steps", u, c[u], s[u]);
+  std::vector<int4> pc;
+  std::vector<int> off;
+  int nq = 0;
+  schedule_queue(c, s, machines, tail, &pc, &off, &nq);
+  if ((int)pc.size() > cap)
+    return fail(GD_EINVAL, "gd_schedule_queue: %zu pieces exceed cap %d", pc.size(), cap);
+  for (size_t k = 0; k < pc.size(); ++k) {
+    pieces[4 * k] = pc[k].x;
+    pieces[4 * k + 1] = pc[k].y;
+    pieces[4 * k + 2] = pc[k].z;
+    pieces[4 * k + 3] = pc[k].w;
+  }
+  for (int k = 0; k <= machines; ++k) piece_off[k] = off[k];
+  *n_queue = nq;
   return GD_OK;
 }
 
@@ -958,6 +993,38 @@ int schedule_pieces(const std::vector<double> &cost, const std::vector<int> &ste
     piece_off->push_back((int)pieces->size());
   }
   return (int)mach.size();
+}
+
+int schedule_queue(const std::vector<double> &cost, const std::vector<int> &steps, int m, int tail,
+                   std::vector<int4> *pieces, std::vector<int> *piece_off, int *n_queue) {
+  const size_t n = cost.size();
+  std::vector<int> head(n);
+  for (size_t u = 0; u < n; ++u) head[u] = std::max(0, steps[u] - std::max(tail, 0));
+  const int used = schedule_pieces(cost, head, m, pieces, piece_off);
+  // when each unit's first part ends, along its machine's list (cost units)
+  std::vector<double> ready(n, 0.0);
+  for (int k = 0; k < used; ++k) {
+    double t = 0.0;
+    for (int q = (*piece_off)[k]; q < (*piece_off)[k + 1]; ++q) {
+      const int4 &pz = (*pieces)[q];
+      t += cost[pz.x] * (pz.z - pz.y);
+      if (pz.z == head[pz.x]) ready[pz.x] = t;
+    }
+  }
+  while ((int)piece_off->size() < m + 1) piece_off->push_back(piece_off->back());
+  std::vector<int> order(n);
+  for (size_t u = 0; u < n; ++u) order[u] = (int)u;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return ready[a] < ready[b]; });
+  *n_queue = 0;
+  for (int j = 0; j < tail; ++j)
+    for (int u : order)
+      if (head[u] + j < steps[u]) {
+        const int lo = head[u] + j;
+        pieces->push_back(make_int4(u, lo, lo + 1, lo > 0 ? 1 : 0));
+        *n_queue += 1;
+      }
+  return m;
 }
 
 }  // namespace gd

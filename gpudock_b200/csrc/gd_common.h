@@ -76,6 +76,7 @@ struct gd_ctx {
   int n_sm = 148;
   int sched_mode = 0;      // GD_SCHED_*
   int sched_machines = 0;  // persistent CTAs (0: SMs x occupancy)
+  int sched_tail = 2;      // last MC steps of every unit left to the shared queue
   int split_mode = 0;      // CTAs per unit of MC launches (0: split_for's rule)
   uint32_t wait_limit = 0; // polls of a dependency wait before it gives up (0: default)
   int wait_bias = 0;       // added to every dependency wait's target (test hook)

@@ -48,9 +48,11 @@ struct Plan {
   int *d_progress = nullptr;      // [grid] MC steps done by each unit
   int auto_machines = 0;          // SMs x resident CTAs per SM (0: not asked yet)
   struct Sched {
-    int n_steps = 0, machines = 0, grid = 0;
+    int n_steps = 0, machines = 0, grid = 0, tail = 0;
+    int n_queue = 0, queue_first = 0;  // the shared queue (KRun.n_queue)
     int4 *d_pieces = nullptr;
     int *d_off = nullptr, *d_ticket = nullptr;
+    int *d_queue_ctl = nullptr;  // [2]: next queue piece, CTAs done
   };
   std::vector<Sched> scheds;
 };
@@ -359,6 +361,14 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
   return R;
 }
 
+// MC steps per unit left to a persistent launch's shared queue: only for a
+// run of one launch plan, whose CTAs then all fit on the GPU at once (a queue
+// piece may wait on any unit's earlier steps, on whichever CTA runs them).
+int sched_tail(const Ens &E, int n_steps) {
+  if (E.plans.size() != 1) return 0;
+  return std::min(E.ctx->sched_tail, n_steps);
+}
+
 // Makes (once per launch length) the persistent schedule of every plan that
 // the context's schedule mode gives one; called outside stream capture.
 gd_status ens_prepare(Ens &E, int n_steps) {
@@ -376,17 +386,28 @@ gd_status ens_prepare(Ens &E, int n_steps) {
     }
     const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
     if (pl.split > 1 || (mode == GD_SCHED_AUTO && pl.grid <= machines)) continue;
+    const int tail = sched_tail(E, n_steps);
     bool have = false;
     for (const Plan::Sched &s : pl.scheds)
-      have = have || (s.n_steps == n_steps && s.machines == machines);
+      have = have || (s.n_steps == n_steps && s.machines == machines && s.tail == tail);
     if (have) continue;
     Plan::Sched s;
     s.n_steps = n_steps;
     s.machines = machines;
+    s.tail = tail;
     std::vector<int4> pieces;
     std::vector<int> off;
-    s.grid = schedule_pieces(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines, &pieces,
-                             &off);
+    if (tail > 0) {
+      // a plan alone on the GPU (all its CTAs resident): each unit's last
+      // steps go to the shared queue
+      s.grid = schedule_queue(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines, tail,
+                              &pieces, &off, &s.n_queue);
+      s.queue_first = off[machines];
+      GD_TRY(dalloc(E, &s.d_queue_ctl, 2));
+    } else {
+      s.grid = schedule_pieces(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines,
+                               &pieces, &off);
+    }
     GD_TRY(dcopy(E, &s.d_pieces, pieces));
     GD_TRY(dcopy(E, &s.d_off, off));
     GD_TRY(dalloc(E, &s.d_ticket, 1));
@@ -402,8 +423,9 @@ const Plan::Sched *find_sched(const Ens &E, const Plan &pl, int n_steps) {
   if (pl.split > 1) return nullptr;  // split plans' staging is per rank: never a schedule
   const int machines = E.ctx->sched_machines ? E.ctx->sched_machines : pl.auto_machines;
   if (mode == GD_SCHED_AUTO && pl.grid <= machines) return nullptr;
+  const int tail = sched_tail(E, n_steps);
   for (const Plan::Sched &s : pl.scheds)
-    if (s.n_steps == n_steps && s.machines == machines) return &s;
+    if (s.n_steps == n_steps && s.machines == machines && s.tail == tail) return &s;
   return nullptr;
 }
 
@@ -433,6 +455,9 @@ gd_status launch_plans(Ens &E, int mode, int step0, int n_steps, bool device_ste
     if (mode == KMODE_REMC) {
       if (const Plan::Sched *sc = find_sched(E, pl, n_steps)) {
         R.pieces = sc->d_pieces;
+        R.n_queue = sc->n_queue;
+        R.queue_first = sc->queue_first;
+        R.queue_ctl = sc->d_queue_ctl;
         R.piece_off = sc->d_off;
         R.ticket = sc->d_ticket;
         R.progress = pl.d_progress;
@@ -453,8 +478,11 @@ gd_status ens_init(Ens &E) {
   cudaStream_t s = E.ctx->stream;
   GD_CUDA(cudaMemsetAsync(E.acs_exchg, 0, sizeof(int) * MAX_TMP * E.items.size(), s));
   GD_CUDA(cudaMemsetAsync(E.d_step, 0, sizeof(int), s));
-  for (const Plan &pl : E.plans)  // progress counts steps from 0 again
+  for (const Plan &pl : E.plans) {  // progress counts steps from 0 again
     GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
+    for (const Plan::Sched &sc : pl.scheds)
+      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 2 * sizeof(int), s));
+  }
   GD_TRY(launch_plans(E, KMODE_INIT, 0, 1, false));
   E.step = 0;
   E.t_compute = 0.0;
@@ -866,8 +894,11 @@ gd_status ens_restore(Ens &E, const void *buf, size_t size) {
   }
   // progress words count absolute steps and only ever grow within a run:
   // start them again below the restored step
-  for (const Plan &pl : E.plans)
+  for (const Plan &pl : E.plans) {
     GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
+    for (const Plan::Sched &sc : pl.scheds)
+      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 2 * sizeof(int), s));
+  }
   GD_CUDA(cudaStreamSynchronize(s));  // the host buffer may be reused on return
   E.step = h.step;
   if (E.traj) E.traj->seq = E.traj->spd > 0 ? h.step / E.traj->spd : 0;

@@ -145,8 +145,14 @@ struct KRun {
   // each {unit, first step, end step, wait}: MC steps [first, end) of the
   // launch for that unit, after waiting (wait != 0) until progress[unit]
   // reaches the launch's first step + first.
+  // With n_queue > 0 a CTA that has run its own pieces takes pieces
+  // queue_first, queue_first + 1, ... (one at a time, in order) from a shared
+  // counter (queue_ctl[0]); the last CTA to find the queue empty (counted in
+  // queue_ctl[1]) sets both back to 0 for the next launch.
   const int4 *pieces;
   const int *piece_off;  // [grid + 1]
+  int n_queue, queue_first;
+  int *queue_ctl;
   int *ticket;           // start-order counter, 0 before the launch (wraps)
   int *progress;         // [units] MC steps done (absolute step count)
   int *err;              // error word: 2 bounded wait ran out, 3 hb_pairs too
@@ -169,6 +175,16 @@ struct KRun {
 // machines that got work.
 int schedule_pieces(const std::vector<double> &cost, const std::vector<int> &steps, int m,
                     std::vector<int4> *pieces, std::vector<int> *piece_off);
+// The same for each unit's first steps[u] - tail steps, plus a shared queue:
+// the last `tail` steps of every unit as one-step pieces, appended after the
+// m machines' pieces (piece_off has m + 1 entries, empty machines included),
+// first every unit's first tail step, then its second, ..., units in the
+// order their first part is expected to end.  CTAs that have run their own
+// pieces take queue pieces in order, so the launch ends within about one
+// unit-step of the balanced length whatever the machines' actual speeds.
+// Returns m, the queue length in *n_queue.
+int schedule_queue(const std::vector<double> &cost, const std::vector<int> &steps, int m, int tail,
+                   std::vector<int4> *pieces, std::vector<int> *piece_off, int *n_queue);
 
 // Atom pairs of warp 0 (the most) holding a slot below n_hb: a warp's pair h
 // holds slots ag + 2hA and ag + (2h+1)A.

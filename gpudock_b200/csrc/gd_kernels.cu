@@ -649,6 +649,28 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
   __syncthreads();
 
   for (;;) {
+  if (PIECES && R.n_queue > 0 && s_ctl->pc >= s_ctl->pc_end) {
+    // this CTA's own pieces are done: the next piece of the shared queue
+    __syncthreads();  // every thread has read s_ctl
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(R.queue_ctl, 1);
+      if (q < R.n_queue) {
+        s_ctl->pc = R.queue_first + q;
+        s_ctl->pc_end = s_ctl->pc + 1;
+      } else {
+        s_ctl->pc = 1;  // none left: the CTA ends
+        s_ctl->pc_end = 0;
+        // the last CTA out sets the queue back for the next launch (every
+        // CTA's last claim is ordered before its count)
+        __threadfence();
+        if (atomicAdd(R.queue_ctl + 1, 1) == (int)gridDim.x - 1) {
+          R.queue_ctl[0] = 0;
+          R.queue_ctl[1] = 0;
+        }
+      }
+    }
+    __syncthreads();
+  }
   const int pc = s_ctl->pc;
   if (pc >= s_ctl->pc_end) break;
   int unit = blockIdx.x / csize, lo = 0, hi = -1;  // hi < 0: every step of the launch

@@ -47,6 +47,7 @@ def _declare(lib):
         "gd_autotune": ([P, P, C.POINTER(abi.GdTile), C.POINTER(C.c_double)], i32),
         "gd_ctx_set_tile": ([P, i32, i32, C.POINTER(abi.GdTile)], i32),
         "gd_ctx_set_schedule": ([P, i32, i32], i32),
+        "gd_ctx_set_schedule_tail": ([P, i32], i32),
         "gd_ctx_set_split": ([P, i32], i32),
         "gd_ctx_set_wait_test": ([P, C.c_uint, i32], i32),
         "gd_ctx_set_alloc_fail": ([P, i32], i32),
@@ -65,6 +66,9 @@ def _declare(lib):
         "gd_schedule_pieces": ([C.POINTER(C.c_double), C.POINTER(C.c_int), i32, i32,
                                 C.POINTER(C.c_int), i32, C.POINTER(C.c_int),
                                 C.POINTER(C.c_int)], i32),
+        "gd_schedule_queue": ([C.POINTER(C.c_double), C.POINTER(C.c_int), i32, i32, i32,
+                               C.POINTER(C.c_int), i32, C.POINTER(C.c_int),
+                               C.POINTER(C.c_int)], i32),
         "gd_batch_create": ([P, i32, C.POINTER(P), C.POINTER(abi.GdMcParams), C.POINTER(P)], i32),
         "gd_batch_init": ([P], i32),
         "gd_batch_run": ([P, i32], i32),
@@ -196,6 +200,11 @@ class Context:
     def set_schedule(self, mode: int, machines: int = 0):
         """abi.SCHED_AUTO / SCHED_WAVES / SCHED_PERSISTENT (over `machines` CTAs)."""
         check(self._lib.gd_ctx_set_schedule(self.h, mode, machines), "gd_ctx_set_schedule")
+
+    def set_schedule_tail(self, tail: int):
+        """MC steps per unit left to a persistent launch's shared queue
+        (gd_ctx_set_schedule_tail; default 2, 0: none)."""
+        check(self._lib.gd_ctx_set_schedule_tail(self.h, tail), "gd_ctx_set_schedule_tail")
 
     def set_wait_test(self, wait_limit: int, never_release: bool):
         """Test hook: dependency waits of later MC launches give up after
@@ -629,6 +638,24 @@ def schedule_pieces(cost, steps, machines: int):
           "gd_schedule_pieces")
     u = used.value
     return pieces[:off[u]].copy(), off[:u + 1].copy()
+
+
+def schedule_queue(cost, steps, machines: int, tail: int):
+    """The persistent schedule with a shared queue: (pieces [n][4], piece_off
+    [machines + 1], n_queue); the queue is the last n_queue pieces."""
+    lib = load()
+    cost = np.ascontiguousarray(cost, np.float64)
+    steps = np.ascontiguousarray(steps, np.int32)
+    n = len(cost)
+    cap = 2 * n + machines + 1 + n * tail
+    pieces = np.zeros((cap, 4), np.int32)
+    off = np.zeros(machines + 1, np.int32)
+    nq = C.c_int(0)
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    check(lib.gd_schedule_queue(cost.ctypes.data_as(C.POINTER(C.c_double)), ip(steps), n,
+                                machines, tail, ip(pieces), cap, ip(off), C.byref(nq)),
+          "gd_schedule_queue")
+    return pieces[:off[machines] + nq.value].copy(), off, nq.value
 
 
 def trajectory_dtype(layout: dict) -> np.dtype:

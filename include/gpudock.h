@@ -335,6 +335,14 @@ gd_status gd_ctx_set_tile(gd_ctx *ctx, int lna, int pnp, const gd_tile *tile);
  * built with). */
 enum { GD_SCHED_AUTO = 0, GD_SCHED_WAVES = 1, GD_SCHED_PERSISTENT = 2 };
 gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
+/* Persistent launches of a run with one launch shape: the last `tail` MC
+ * steps of every unit (default 2; 0: none) are not dealt to the CTAs in
+ * advance but left in a queue, one step per piece, that CTAs which have run
+ * their own share take from in order.  The CTAs then end within about one
+ * unit-step of each other even when units or SMs run at different speeds
+ * (contacts, clocks).  Trajectories stay bit-identical.  Applies to runs
+ * whose schedule is made after the call. */
+gd_status gd_ctx_set_schedule_tail(gd_ctx *ctx, int tail);
 
 /* How many CTAs share each 32-replica unit of an MC launch.  With split > 1
  * the unit runs on a thread-block cluster of `split` CTAs (SMs of one GPC):
@@ -684,6 +692,13 @@ gd_status gd_ctx_set_alloc_fail(gd_ctx *ctx, int nth);
 gd_status gd_schedule_pieces(const double *cost, const int *steps, int n_units,
                              int machines, int *pieces, int cap, int *piece_off,
                              int *n_used);
+/* The persistent schedule with a shared queue (host only): the first
+ * steps[u] - tail steps of every unit cut as by gd_schedule_pieces over
+ * `machines` CTAs (piece_off: machines + 1 entries), followed by *n_queue
+ * one-step pieces {unit, step, step + 1, wait} (the last `tail` steps of every
+ * unit, step by step, units in the order their first part ends). */
+gd_status gd_schedule_queue(const double *cost, const int *steps, int n_units, int machines,
+                            int tail, int *pieces, int cap, int *piece_off, int *n_queue);
 
 #ifdef __cplusplus
 }

@@ -29,8 +29,9 @@ def _same(a, b):
         assert np.array_equal(a.record, b.record)
 
 
-def _remc(ctx, d, mb, steps, spe, flags, chunks, sched, machines=0):
+def _remc(ctx, d, mb, steps, spe, flags, chunks, sched, machines=0, tail=2):
     ctx.set_schedule(sched, machines)
+    ctx.set_schedule_tail(tail)
     r = lib.Remc(d, steps, spe, mb, seed=21, flags=flags)
     r.init()
     for n in chunks:
@@ -57,10 +58,12 @@ def test_persistent_equals_waves(ctx, case):
     _, mb = lib.set_temperature(n_tmp, 0.004, 0.04)
     steps, spe = 40, 10
     ref = _remc(ctx, d, mb, steps, spe, flags, [20, 20], abi.SCHED_WAVES)
-    for machines in (1, 2, 3, 5):
-        got = _remc(ctx, d, mb, steps, spe, flags, [20, 20], abi.SCHED_PERSISTENT, machines)
+    # tail > 0: the last steps of every unit go through the shared queue
+    for machines, tail in ((1, 2), (2, 0), (2, 1), (3, 2), (5, 5), (5, 0)):
+        got = _remc(ctx, d, mb, steps, spe, flags, [20, 20], abi.SCHED_PERSISTENT, machines, tail)
         _same(got, ref)
     ctx.set_schedule(abi.SCHED_AUTO)
+    ctx.set_schedule_tail(2)
 
 
 def test_persistent_batch_of_items(ctx):
@@ -81,8 +84,9 @@ def test_persistent_batch_of_items(ctx):
     params = [abi.mc_params(steps, spe, mb, seed=4, stream_id=i, flags=flags)
               for i in range(len(cxs))]
 
-    def run(sched, machines=0):
+    def run(sched, machines=0, tail=2):
         ctx.set_schedule(sched, machines)
+        ctx.set_schedule_tail(tail)
         b = lib.Batch(ctx, dcxs, params)
         b.init()
         b.run(steps)
@@ -91,10 +95,11 @@ def test_persistent_batch_of_items(ctx):
         return out
 
     ref = run(abi.SCHED_WAVES)
-    for machines in (1, 3, 7):
-        for a, b in zip(run(abi.SCHED_PERSISTENT, machines), ref):
+    for machines, tail in ((1, 2), (3, 0), (3, 3), (7, 2)):
+        for a, b in zip(run(abi.SCHED_PERSISTENT, machines, tail), ref):
             _same(a, b)
     ctx.set_schedule(abi.SCHED_AUTO)
+    ctx.set_schedule_tail(2)
 
 
 def test_schedule_option_checks(ctx):

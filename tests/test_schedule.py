@@ -83,3 +83,54 @@ def test_edges():
         lib.schedule_pieces([1.0], [3], 0)
     with pytest.raises(lib.GdError):
         lib.schedule_pieces([0.0], [3], 2)
+
+
+def _check_queue(cost, steps, m, tail):
+    """Schedules with a shared queue: the machines' pieces cover each unit's
+    first steps[u] - tail steps (as the plain schedule does), the queue holds
+    each remaining step once as a one-step piece, a unit's queue steps come in
+    order and after its own machine part, and every piece but a unit's first
+    waits."""
+    pieces, off, nq = lib.schedule_queue(cost, steps, m, tail)
+    assert len(off) == m + 1 and off[m] + nq == len(pieces)
+    head = [max(0, s - tail) for s in steps]
+    static, queue = pieces[:off[m]], pieces[off[m]:]
+    ref, ref_off = lib.schedule_pieces(cost, head, m)
+    assert np.array_equal(static, ref)
+    assert np.array_equal(off[:len(ref_off)], ref_off) and (off[len(ref_off) - 1:] == ref_off[-1]).all()
+    assert (queue[:, 2] - queue[:, 1] == 1).all()
+    assert np.array_equal(queue[:, 3] != 0, queue[:, 1] > 0)
+    assert np.array_equal(static[:, 3] != 0, static[:, 1] > 0)
+    for u, n in enumerate(steps):
+        q = queue[queue[:, 0] == u, 1]
+        assert list(q) == list(range(head[u], n))
+    # the queue takes every unit's first queued step before any unit's second
+    rank = np.array([s - head[u] for u, s in queue[:, :2]])
+    assert (np.diff(rank) >= 0).all()
+    return pieces, off, nq
+
+
+def test_queue_ensemble():
+    # 275 units of 20 steps on 148 CTAs, the last 2 steps of each in the queue
+    pieces, off, nq = _check_queue([1.0] * 275, [20] * 275, 148, 2)
+    assert nq == 550
+    per = np.diff(off)
+    assert per.min() >= 1
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_queue_random(seed):
+    rng = np.random.default_rng(200 + seed)
+    n = int(rng.integers(1, 300))
+    cost = rng.uniform(0.2, 5.0, n)
+    steps = rng.integers(0, 30, n)
+    _check_queue(cost, steps, int(rng.integers(1, 200)), int(rng.integers(0, 5)))
+
+
+def test_queue_edges():
+    _check_queue([1.0], [1], 8, 2)       # the whole unit in the queue
+    _check_queue([1.0] * 3, [2] * 3, 2, 2)
+    pieces, off, nq = _check_queue([1.0] * 5, [10] * 5, 3, 0)
+    assert nq == 0
+    with pytest.raises(lib.GdError):
+        lib.schedule_queue([1.0], [3], 2, -1)
