@@ -52,7 +52,7 @@ struct Plan {
     int n_queue = 0, queue_first = 0;  // the shared queue (KRun.n_queue)
     int4 *d_pieces = nullptr;
     int *d_off = nullptr, *d_ticket = nullptr;
-    int *d_queue_ctl = nullptr;  // [2]: next queue piece, CTAs done
+    int *d_queue_ctl = nullptr;  // [3]: next queue piece, CTAs done, CTAs started
   };
   std::vector<Sched> scheds;
 };
@@ -362,8 +362,8 @@ KRun run_desc(const Ens &E, const Plan &pl, int mode) {
 }
 
 // MC steps per unit left to a persistent launch's shared queue: only for a
-// run of one launch plan, whose CTAs then all fit on the GPU at once (a queue
-// piece may wait on any unit's earlier steps, on whichever CTA runs them).
+// run of one launch plan, whose CTAs then normally all fit on the GPU at once
+// (CTAs take queue pieces only once all of them have started).
 int sched_tail(const Ens &E, int n_steps) {
   if (E.plans.size() != 1) return 0;
   return std::min(E.ctx->sched_tail, n_steps);
@@ -403,7 +403,7 @@ gd_status ens_prepare(Ens &E, int n_steps) {
       s.grid = schedule_queue(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines, tail,
                               &pieces, &off, &s.n_queue);
       s.queue_first = off[machines];
-      GD_TRY(dalloc(E, &s.d_queue_ctl, 2));
+      GD_TRY(dalloc(E, &s.d_queue_ctl, 3));
     } else {
       s.grid = schedule_pieces(pl.unit_cost, std::vector<int>(pl.grid, n_steps), machines,
                                &pieces, &off);
@@ -481,7 +481,7 @@ gd_status ens_init(Ens &E) {
   for (const Plan &pl : E.plans) {  // progress counts steps from 0 again
     GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
     for (const Plan::Sched &sc : pl.scheds)
-      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 2 * sizeof(int), s));
+      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 3 * sizeof(int), s));
   }
   GD_TRY(launch_plans(E, KMODE_INIT, 0, 1, false));
   E.step = 0;
@@ -897,7 +897,7 @@ gd_status ens_restore(Ens &E, const void *buf, size_t size) {
   for (const Plan &pl : E.plans) {
     GD_CUDA(cudaMemsetAsync(pl.d_progress, 0, sizeof(int) * std::max(pl.grid, 1), s));
     for (const Plan::Sched &sc : pl.scheds)
-      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 2 * sizeof(int), s));
+      if (sc.d_queue_ctl) GD_CUDA(cudaMemsetAsync(sc.d_queue_ctl, 0, 3 * sizeof(int), s));
   }
   GD_CUDA(cudaStreamSynchronize(s));  // the host buffer may be reused on return
   E.step = h.step;

@@ -147,8 +147,9 @@ struct KRun {
   // reaches the launch's first step + first.
   // With n_queue > 0 a CTA that has run its own pieces takes pieces
   // queue_first, queue_first + 1, ... (one at a time, in order) from a shared
-  // counter (queue_ctl[0]); the last CTA to find the queue empty (counted in
-  // queue_ctl[1]) sets both back to 0 for the next launch.
+  // counter (queue_ctl[0]), once every CTA of the launch has started
+  // (queue_ctl[2] counts them); the last CTA to leave (counted in
+  // queue_ctl[1]) sets all three back to 0 for the next launch.
   const int4 *pieces;
   const int *piece_off;  // [grid + 1]
   int n_queue, queue_first;

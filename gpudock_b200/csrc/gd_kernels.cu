@@ -638,6 +638,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       const int m = (int)atomicInc(reinterpret_cast<unsigned *>(R.ticket), gridDim.x - 1);
       pc = R.piece_off[m];
       pc_end = R.piece_off[m + 1];
+      if (R.n_queue > 0) atomicAdd(R.queue_ctl + 2, 1);  // CTAs started
     }
     s_ctl->pc = pc;
     s_ctl->pc_end = pc_end;
@@ -653,7 +654,11 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
     // this CTA's own pieces are done: the next piece of the shared queue
     __syncthreads();  // every thread has read s_ctl
     if (threadIdx.x == 0) {
-      const int q = atomicAdd(R.queue_ctl, 1);
+      // queue pieces may wait on any CTA's pieces: take them only once every
+      // CTA of the launch has started (else this CTA leaves the queue to the
+      // later ones), so that every wait is on a running CTA
+      const bool all_started = ld_acquire(R.queue_ctl + 2) >= (int)gridDim.x;
+      const int q = all_started ? atomicAdd(R.queue_ctl, 1) : R.n_queue;
       if (q < R.n_queue) {
         s_ctl->pc = R.queue_first + q;
         s_ctl->pc_end = s_ctl->pc + 1;
@@ -666,6 +671,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
         if (atomicAdd(R.queue_ctl + 1, 1) == (int)gridDim.x - 1) {
           R.queue_ctl[0] = 0;
           R.queue_ctl[1] = 0;
+          R.queue_ctl[2] = 0;
         }
       }
     }
