@@ -398,7 +398,7 @@ def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool
            for i, (n, k) in enumerate(zip(lnas, which))]
     _, mb = synth.temperatures(w)
     srv = lib.Server(0, hbm_budget_bytes=int(budget_gb) << 30, max_active=max_active,
-                     steps_per_launch=steps_per_launch or w.steps_per_exchange * 10)
+                     steps_per_launch=steps_per_launch or w.steps_per_exchange * 2)
     if split is not None:
         srv.set_split(split)
     pids = [srv.add_protein(cxs[int(np.nonzero(which == k)[0][0])]) if (which == k).any()

@@ -604,7 +604,10 @@ gd_status gd_batch_kernel_times(gd_batch *batch, double *mc_ms, int *mc_launches
 /* active request (ligand atoms x protein points) advances steps_per_launch */
 /* MC steps (at least one exchange interval) and cheaper ones               */
 /* proportionally more, in whole exchange intervals, so that no request     */
-/* holds the others back.                                                   */
+/* holds the others back.  Short iterations keep the SMs busier: on the     */
+/* serving trace (10-step exchange interval) 20 steps per launch served     */
+/* 63.8 req/s at SM occupancy 0.86, against 60.2 / 0.81 with 100 and        */
+/* 54.8 / 0.74 with 400.                                                    */
 /* ------------------------------------------------------------------------ */
 typedef struct gd_server gd_server;
 
