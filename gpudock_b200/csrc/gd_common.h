@@ -140,7 +140,7 @@ Tile tile_for(gd_ctx *ctx, const KTables &T);
 // request is a run of its own among others and splits only from
 // kServeSplitCost, so that splitting under load costs little throughput.
 constexpr double kRunSplitCost = 4500.0;
-constexpr double kServeSplitCost = 85000.0;
+constexpr double kServeSplitCost = 42500.0;
 int split_for(gd_ctx *ctx, const KTables &T, int run_units, double min_cost);
 // 32-replica units of a complex's replicas (n_prt x n_lig x n_tmp): whole
 // exchange groups per unit when n_tmp divides 32.

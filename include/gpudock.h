@@ -355,10 +355,10 @@ gd_status gd_ctx_set_schedule_tail(gd_ctx *ctx, int tail);
  * protein points / c and <= SMs / units of the run, at most 8, with
  * c = 4,500 for runs and batches (they have the GPU to themselves: a
  * 24-atom ligand against 1,500 points runs on 8 CTAs, an ensemble or batch
- * with more units than SMs unsplit) and c = 85,000 for server requests
+ * with more units than SMs unsplit) and c = 42,500 for server requests
  * (each a run of its own among others, so that splitting under load costs
  * little throughput: 120 atoms against 10,000 points on 8 CTAs, 30 atoms
- * against 4,000 unsplit); 1, 2, 4 or 8 fix it for every complex.  A run's
+ * against 4,000 on 2); 1, 2, 4 or 8 fix it for every complex.  A run's
  * results depend on its split (the partial sums are added in another
  * order) but never on what runs beside it.  Applies to runs, batches and
  * server lanes created after the call. */
