@@ -206,15 +206,8 @@ __device__ __forceinline__ int hpc_pair_at(int g, int ag, int h, int lane, int A
 // group ag: the P tile groups' sums of the pair's two slots added in group
 // order, then 0.5 hh^2 - hpl2 with hh = (sum - hpl0) / hpl1 for each slot
 // that holds an atom (0 for a slot past the ligand).
-__device__ __forceinline__ float2 hpc_restraint(const KTables &T, const float2 *s_hpc2,
-                                                const int *s_lt, int P, int A, int NH, int ag,
-                                                int hp, int lane) {
-  float2 v = make_float2(0.f, 0.f);
-  for (int g = 0; g < P; ++g) {
-    const float2 x = s_hpc2[hpc_pair_at(g, ag, hp, lane, A, NH)];
-    v.x += x.x;
-    v.y += x.y;
-  }
+__device__ __forceinline__ float2 hpc_transform(const KTables &T, const int *s_lt, int A, int ag,
+                                                int hp, float2 v) {
   float r[2] = {0.f, 0.f};
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -226,6 +219,17 @@ __device__ __forceinline__ float2 hpc_restraint(const KTables &T, const float2 *
     }
   }
   return make_float2(r[0], r[1]);
+}
+__device__ __forceinline__ float2 hpc_restraint(const KTables &T, const float2 *s_hpc2,
+                                                const int *s_lt, int P, int A, int NH, int ag,
+                                                int hp, int lane) {
+  float2 v = make_float2(0.f, 0.f);
+  for (int g = 0; g < P; ++g) {
+    const float2 x = s_hpc2[hpc_pair_at(g, ag, hp, lane, A, NH)];
+    v.x += x.x;
+    v.y += x.y;
+  }
+  return hpc_transform(T, s_lt, A, ag, hp, v);
 }
 
 // Warp 0 after the step's partial sums: cross-warp reduction in a fixed
@@ -1106,46 +1110,51 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 1)
       // no CTA passes before it has read this step's buffers.
       unsigned char *xb = smem + SL.xch + (size_t)(si & 1) * SL.xch_step;
       double *xs = reinterpret_cast<double *>(xb);
-      float *xh = reinterpret_cast<float *>(xb + (size_t)NRED * 32 * sizeof(double));
-      if (warp == 0) {
-        for (int i = 0; i < NRED; ++i) {
+      float2 *xh2 = reinterpret_cast<float2 *>(xb + (size_t)NRED * 32 * sizeof(double));
+      float2 *s_hpc2 = reinterpret_cast<float2 *>(s_hpc);
+      // both halves spread over the warps (tasks i = lw, lw + W, ... of the
+      // NRED terms and the A x NH atom pairs, each summed in a fixed order):
+      // this CTA's sums over its warp slots and tile groups into the buffer
+      for (int i = lw; i < NRED + A * NH; i += W) {
+        if (i < NRED) {
           double acc = 0.0;
           for (int w = 0; w < W; ++w) acc += s_red[((size_t)w * NRED + i) * 32 + lane];
           xs[i * 32 + lane] = acc;
-        }
-        const float2 *s_hpc2 = reinterpret_cast<const float2 *>(s_hpc);
-        float2 *xh2 = reinterpret_cast<float2 *>(xh);
-        for (int i = 0; i < A * NH; ++i) {  // atom pairs (ag, h) = (i / NH, i % NH)
+        } else {
+          const int j = i - NRED;  // atom pair (ag, h) = (j / NH, j % NH)
           float2 v = make_float2(0.f, 0.f);
           for (int g = 0; g < P; ++g) {
-            const float2 x = s_hpc2[hpc_pair_at(g, i / NH, i % NH, lane, A, NH)];
+            const float2 x = s_hpc2[hpc_pair_at(g, j / NH, j % NH, lane, A, NH)];
             v.x += x.x;
             v.y += x.y;
           }
-          xh2[i * 32 + lane] = v;
+          xh2[j * 32 + lane] = v;
         }
       }
       cluster_sync_all();
-      if (warp == 0) {
-        for (int i = 0; i < NRED; ++i) {
+      // then all ranks' buffers in rank order into slot 0 (terms) and tile
+      // group 0's slots (the atom pairs' hydrophobic restraints)
+      for (int i = lw; i < NRED + A * NH; i += W) {
+        if (i < NRED) {
           double acc = 0.0;
           for (int r = 0; r < csize; ++r) acc += cluster_map(xs, r)[i * 32 + lane];
-          s_red[(size_t)i * 32 + lane] = acc;  // warp 0's slots
-        }
-        float2 *s_hpc2 = reinterpret_cast<float2 *>(s_hpc);
-        const float2 *xh2 = reinterpret_cast<const float2 *>(xh);
-        for (int i = 0; i < A * NH; ++i) {
+          s_red[(size_t)i * 32 + lane] = acc;
+        } else {
+          const int j = i - NRED, ai = j / NH, hp = j % NH;
           float2 v = make_float2(0.f, 0.f);
           for (int r = 0; r < csize; ++r) {
-            const float2 x = cluster_map(xh2, r)[i * 32 + lane];
+            const float2 x = cluster_map(xh2, r)[j * 32 + lane];
             v.x += x.x;
             v.y += x.y;
           }
-          s_hpc2[hpc_pair_at(0, i / NH, i % NH, lane, A, NH)] = v;  // tile group 0's
+          if (ai + 2 * hp * A < lna)
+            s_hpc2[hpc_pair_at(0, ai, hp, lane, A, NH)] = hpc_transform(T, s_lt, A, ai, hp, v);
         }
-        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, A, NH, lane, rep, active, prt_conf,
-                          lig_conf, step, crank0 == 0, false);
       }
+      named_sync(1, W * 32);
+      if (warp == 0)
+        finish_step<MODE>(R, I, me, s_red, s_hpc, s_lt, 1, 1, A, NH, lane, rep, active, prt_conf,
+                          lig_conf, step, crank0 == 0, true);
     } else {
       // spread over the warps (tasks i = lw, lw + W, ...): the cross-warp sum
       // of each of the NRED terms (in warp-slot order, into slot 0) and the
