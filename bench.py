@@ -397,8 +397,9 @@ def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool
                               seed=seed + 1000 + i, protein=prots[k])
            for i, (n, k) in enumerate(zip(lnas, which))]
     _, mb = synth.temperatures(w)
+    steps_per_launch = steps_per_launch or w.steps_per_exchange * 2
     srv = lib.Server(0, hbm_budget_bytes=int(budget_gb) << 30, max_active=max_active,
-                     steps_per_launch=steps_per_launch or w.steps_per_exchange * 2)
+                     steps_per_launch=steps_per_launch)
     if split is not None:
         srv.set_split(split)
     pids = [srv.add_protein(cxs[int(np.nonzero(which == k)[0][0])]) if (which == k).any()
@@ -477,6 +478,7 @@ def form_served(seed, rate=50.0, n_request=2000, steps=2000, budget_gb=120, pool
            "sm_occupancy": st.cta_busy_s / (n_sm * wall),
            "host_launch_s": st.host_launch_s,
            "busy_s": st.busy_s, "launches": st.launches,
+           "steps_per_launch": steps_per_launch,
            "queue_series": {"every_s": 0.5, "columns": ["t_s", "queued", "active", "completed"],
                             "rows": series[::4]},
            "sample": f"{n_request} requests of the 10,000-request trace at {rate:g} req/s, "
