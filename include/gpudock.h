@@ -338,10 +338,11 @@ gd_status gd_ctx_set_schedule(gd_ctx *ctx, int mode, int machines);
 /* Persistent launches of a run with one launch shape: the last `tail` MC
  * steps of every unit (default 2; 0: none) are not dealt to the CTAs in
  * advance but left in a queue, one step per piece, that CTAs which have run
- * their own share take from in order.  The CTAs then end within about one
- * unit-step of each other even when units or SMs run at different speeds
- * (contacts, clocks).  Trajectories stay bit-identical.  Applies to runs
- * whose schedule is made after the call. */
+ * their own share take from in order, once every CTA of the launch has
+ * started.  The CTAs then end within about one unit-step of each other even
+ * when units or SMs run at different speeds (contacts, clocks).  Trajectories
+ * stay bit-identical.  Applies to runs whose schedule is made after the call;
+ * tail is 0..64. */
 gd_status gd_ctx_set_schedule_tail(gd_ctx *ctx, int tail);
 
 /* How many CTAs share each 32-replica unit of an MC launch.  With split > 1
